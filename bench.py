@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the exact Fock sampler on B200: samples/s at n = 20, m = 400 (2 000 shots per step,
+lossless, Haar-random U), mixed-precision form against the FP64 form, with the marginal error of the
+mixed form against the FP64 form on the same chains.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference]
+
+A step is one pass of the sampling path over one batch: sigma and per-step seeds drawn from the device
+generator, then the whole chains of all 2 000 shots in one launch of the persistent chain kernel.
+`value` times K steps with inputs resident in HBM (L2 flushed between steps by a 256 MiB write);
+`e2e` times the public `fock_sample` call with U copied from pinned host memory and the occupations
+copied back every step.  Under torchrun every rank runs its own replica (weak scaling, no collective
+on the data path); the time is the max over ranks.  `--impl reference` times the CPU restatement of the
+reference's algorithm (oracle/, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_PHOT, M_MODES, SHOTS, USEED = 20, 400, 2000, 1002
+METRIC = "samples/s n=20 m=400: mixed-precision vs FP64 on B200, marginal err<=1e-6"
+WORKLOAD = "fock n=20 photons (modes 0..19), m=400, 2000 shots/step, lossless, Haar U (seeded QR)"
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ----------------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        except (OSError, ValueError):
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------------------- reference arm
+def run_reference(args):
+    """The CPU restatement of the reference's algorithm (oracle/, C, all host threads) on a bounded sample:
+    every step samples `--ref-shots` chains of the benchmark workload."""
+    ws, rank, _ = _dist()
+    if rank != 0:
+        return
+    import numpy as np
+
+    from oracle import oracle as O
+    U = O.haar_unitary(M_MODES, USEED)
+    A = U[:, :N_PHOT]
+    threads = os.cpu_count() or 1
+    rng = np.random.default_rng(0)
+    S = args.ref_shots or 32 * threads          # about 4-5 s of work per step on this port
+
+    def step():
+        sig = np.argsort(rng.random((S, N_PHOT)), axis=1)
+        u = rng.random((S, N_PHOT))
+        O.chain(A, np.zeros(S, np.int64), sig, u, threads=threads)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = args.steps * S / dt
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": N_PHOT, "m": M_MODES, "shots_per_step": S},
+            "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "port",
+                             "sample": f"{S} chains per step of the n=20 m=400 workload (bounded sample)"},
+            "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------------------- B200 arm
+def run_b200(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from photonic_engines_b200 import _native as NAT
+    from photonic_engines_b200.clifford import fock_sample
+    from photonic_engines_b200.clifford.kernels import chain, pack_instances
+    from photonic_engines_b200.clifford.work import chain_work
+
+    ws, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if ws > 1:
+        dist.init_process_group("nccl", device_id=dev)
+    g = torch.Generator().manual_seed(USEED)
+    z = torch.randn(M_MODES, M_MODES, generator=g, dtype=torch.float64) + 1j * torch.randn(
+        M_MODES, M_MODES, generator=g, dtype=torch.float64)
+    q, r = torch.linalg.qr(z)
+    d = torch.diagonal(r)
+    U_host = (q * (d / d.abs()).unsqueeze(0)).contiguous()
+    U = U_host.to(dev)
+    in_modes = list(range(N_PHOT))
+    acol, off, mm, nn = pack_instances(U, in_modes)
+    dp = torch.zeros(SHOTS, dtype=torch.int64, device=dev)
+    gen = torch.Generator(device=dev).manual_seed(1000 + rank)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    rows_buf = torch.empty(SHOTS, N_PHOT, dtype=torch.int64, device=dev)
+    occ_buf = torch.empty(SHOTS, M_MODES, dtype=torch.int64, device=dev)
+
+    def step(precision, marg=None):
+        sig = torch.argsort(torch.rand(SHOTS, N_PHOT, generator=gen, device=dev), dim=1)
+        seeds = torch.randint(0, 2 ** 31 - 1, (N_PHOT,), generator=gen, device=dev)
+        rows, _, mg = chain(acol, off, mm, nn, dp, sig, m_max=M_MODES, seeds=seeds, precision=precision,
+                            want_marg=marg is not None, check_status=False,
+                            out=(rows_buf, occ_buf, marg) if marg is not None else (rows_buf, occ_buf, None))
+        return sig, seeds, rows
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(precision, steps, warmup):
+        for _ in range(warmup):
+            step(precision)
+        torch.cuda.synchronize(dev)
+        kern_ms, work, all_rows = [], [], []
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        evs = []
+        with ClockSampler(local) as clk:
+            e0.record()
+            for _ in range(steps):
+                flush.fill_(1)
+                sig = torch.argsort(torch.rand(SHOTS, N_PHOT, generator=gen, device=dev), dim=1)
+                seeds = torch.randint(0, 2 ** 31 - 1, (N_PHOT,), generator=gen, device=dev)
+                k0 = torch.cuda.Event(enable_timing=True)
+                k1 = torch.cuda.Event(enable_timing=True)
+                k0.record()
+                rows, _, _ = chain(acol, off, mm, nn, dp, sig, m_max=M_MODES, seeds=seeds, precision=precision,
+                                   want_occ=True, check_status=False)
+                k1.record()
+                evs.append((k0, k1))
+                all_rows.append(rows)
+            e1.record()
+            torch.cuda.synchronize(dev)
+        barrier()
+        elapsed = e0.elapsed_time(e1) * 1e-3
+        kern_ms = [a.elapsed_time(b) for a, b in evs]
+        wk = [chain_work(r.cpu().numpy(), M_MODES) for r in all_rows]
+        return {"elapsed": max_over_ranks(elapsed), "kern_ms": kern_ms, "work": wk, "clocks": clk.summary()}
+
+    peak64 = NAT.pipe_peak_tflops("f64", dev)
+    peak32 = NAT.pipe_peak_tflops("mixed", dev)
+    res = {}
+    for precision in ("f64", "mixed"):
+        res[precision] = timed(precision, args.steps, args.warmup)
+
+    # marginal error of the mixed form against the FP64 form on the same chains (same sigma, same seeds)
+    sig = torch.argsort(torch.rand(256, N_PHOT, generator=gen, device=dev), dim=1)
+    seeds = torch.randint(0, 2 ** 31 - 1, (N_PHOT,), generator=gen, device=dev)
+    dp256 = torch.zeros(256, dtype=torch.int64, device=dev)
+    r64, _, m64 = chain(acol, off, mm, nn, dp256, sig, m_max=M_MODES, seeds=seeds, precision="f64", want_marg=True)
+    rmx, _, mmx = chain(acol, off, mm, nn, dp256, sig, m_max=M_MODES, seeds=seeds, precision="mixed", want_marg=True)
+    max_err = float(((mmx - m64).abs().amax(dim=2) / m64.abs().amax(dim=2)).max())
+    picks_equal = bool(torch.equal(r64, rmx))
+
+    # end to end through the public API: U from pinned host memory, occupations back to the host
+    U_pin = U_host.pin_memory()
+    out_pin = torch.empty(SHOTS, M_MODES, dtype=torch.int64).pin_memory()
+    gen_e2e = torch.Generator(device=dev).manual_seed(7 + rank)
+
+    def e2e_step():
+        Ud = U_pin.to(dev, non_blocking=True)
+        occ = fock_sample(Ud, in_modes, SHOTS, generator=gen_e2e, precision="mixed")
+        out_pin.copy_(occ, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    barrier()
+    ee0, ee1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ee0.record()
+    for _ in range(args.steps):
+        e2e_step()
+    ee1.record()
+    torch.cuda.synchronize(dev)
+    e2e_elapsed = max_over_ranks(ee0.elapsed_time(ee1) * 1e-3)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.ref_shots or 96 * (os.cpu_count() or 1))
+
+    if rank == 0:
+        mx, f64 = res["mixed"], res["f64"]
+
+        def roof(r, peak, unit_bound):
+            flops_launch = statistics.mean(w["flops"] for w in r["work"])
+            dur = statistics.mean(r["kern_ms"]) * 1e-3
+            achieved = flops_launch / dur / 1e12
+            return {"bound": unit_bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": None,
+                    "peak_source": "measured live by pe_pipe_probe (FMA chains) on this GPU",
+                    "flops_per_launch": flops_launch, "launch_ms": dur * 1e3}
+
+        value = ws * SHOTS * args.steps / mx["elapsed"]
+        v64 = ws * SHOTS * args.steps / f64["elapsed"]
+        line = {
+            "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mx["elapsed"] / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 Gray blocks + f64 sums/marginal/CDF",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": N_PHOT, "m": M_MODES, "shots_per_step": SHOTS,
+                       "precision": "mixed", "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": roof(mx, peak32, "fp32"),
+            "fp64": {"value": v64, "ms_per_step": f64["elapsed"] / args.steps * 1e3,
+                     "roofline": roof(f64, peak64, "fp64"), "clocks": f64["clocks"]},
+            "mixed_over_fp64": value / v64,
+            "max_marginal_rel_err": max_err, "picks_equal_fp64": picks_equal,
+            "addends_per_sample": statistics.mean(w["addends"] for w in mx["work"]) / SHOTS,
+            "cpu_baseline": cpu,
+            "e2e": {"value": ws * SHOTS * args.steps / e2e_elapsed, "unit": "samples/s",
+                    "h2d_bytes_per_step": U_host.numel() * 16, "d2h_bytes_per_step": SHOTS * M_MODES * 8},
+            "clocks": mx["clocks"],
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+def cpu_baseline(S: int) -> dict:
+    """The oracle (C restatement of the reference algorithm) on the host cores, bounded sample."""
+    import numpy as np
+
+    from oracle import oracle as O
+    U = O.haar_unitary(M_MODES, USEED)
+    rng = np.random.default_rng(1)
+    threads = os.cpu_count() or 1
+    sig = np.argsort(rng.random((S, N_PHOT)), axis=1)
+    u = rng.random((S, N_PHOT))
+    t0 = time.perf_counter()
+    O.chain(U[:, :N_PHOT], np.zeros(S, np.int64), sig, u, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": S / dt, "unit": "samples/s", "cores": threads, "kind": "port",
+            "sample": f"{S} chains of the n=20 m=400 workload, oracle/ C port, {threads} threads, {dt:.1f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--ref-shots", type=int, default=0, help="chains per CPU sample (0: scaled to the cores)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,114 @@
+/*
+ * pe_b200.h — C ABI of the B200 (sm_100a) Clifford & Clifford Fock sampler.
+ *
+ * Plain pointers and sizes only.  Every pointer named `d_*` is DEVICE memory owned by the caller;
+ * every call is asynchronous on the caller's `stream` (cudaStream_t passed as void*) and returns a
+ * status (0 = launched, < 0 = rejected before launch, see PE_ERR_*).  Errors found inside a kernel
+ * (an out-of-range index that the host did not catch) are written to the device status word of the
+ * workspace and read back with pe_read_status().  Nothing here allocates device memory: the caller
+ * passes a workspace of pe_chain_workspace_bytes() bytes.
+ *
+ * Layout of the circuit data (one "instance" = the input columns of one circuit):
+ *   d_acol      complex128 as interleaved float64 pairs, instance g occupies
+ *               d_acol[2 * (inst_off[g] + j * inst_m[g] + rho)]  for input column j < inst_n[g] and
+ *               output mode rho < inst_m[g]  (column-major: one input column = inst_m[g] contiguous
+ *               complex values, so a marginal reads coalesced rows).
+ *   d_inst_off  int64 [G] element offsets, d_inst_m / d_inst_n int32 [G].
+ * Per stream s (a stream = one shot's chain):
+ *   d_dp        int64 [S] instance of stream s
+ *   d_nk        int32 [S] photons of stream s (<= n_stride), NULL = n_stride for every stream
+ *   d_cols      int64 [S][n_stride] input columns in chain order (sigma applied; indices < inst_n)
+ *   d_uniforms  float64 [S][n_stride] per-step uniforms in [0, 1), or NULL to draw them with
+ *               Philox4x32-10 exactly as the reference's draw kernel does:
+ *               u = (r0 + r1 2^-24) / (1 + 2^-24), r_i = tl.rand(seed, 2 off + i), with
+ *               seed = d_seeds[seed_row[s] * n_stride + k] and off = d_rng_off[s]
+ *   d_seed_row  int64 [S] (NULL = 0), d_rng_off int64 [S] (NULL = s)
+ *   d_order     int64 [S] processing order of the streams (a permutation; NULL = 0..S-1): put the
+ *               longest chains first for a short tail
+ * Outputs:
+ *   d_rows      int64 [S][n_stride] output modes in chain order (entries past nk[s] untouched)
+ *   d_occ       int64 [S][occ_stride] occupations (row s fully written: zeros then counts), or NULL
+ *   d_marg      float64 [S][n_stride][marg_stride] normalised weights w / sum(w) of every step, or NULL
+ */
+#ifndef PE_B200_H
+#define PE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PE_OK 0
+#define PE_ERR_ARG (-1)        /* a NULL pointer, a negative size, an unknown precision */
+#define PE_ERR_SIZE (-2)       /* a size beyond the compiled limits (photons, modes, workspace) */
+#define PE_ERR_CUDA (-3)       /* a CUDA runtime error at launch */
+#define PE_ERR_DEVICE (-4)     /* an index error found on the device (see pe_read_status) */
+
+#define PE_PRECISION_F64 0     /* complex FP64 throughout: the drop-in form */
+#define PE_PRECISION_MIXED 1   /* FP32 Gray blocks, FP64 cross-block sum, FP64 marginal and CDF */
+
+#define PE_MAX_PHOTONS 32      /* photons per stream (cofactor tiers up to 32 columns) */
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int pe_version(void);
+
+/* Largest supported number of output modes for the given block size (shared-memory bound). */
+int pe_max_modes(int block_threads);
+
+/* Bytes of device workspace that pe_fock_chain needs (16-byte aligned pointer). */
+size_t pe_chain_workspace_bytes(int64_t S);
+
+/*
+ * The whole Clifford & Clifford chain of S streams in ONE persistent kernel launch: per stream and
+ * per step k = 1..nk[s], the Laplace cofactors of the chosen-rows block by the collapsed
+ * (2020) Glynn Gray sum, the marginal over all output modes and the inverse-CDF pick.
+ *
+ * Replaces, for the lossless and the lossy/partially-distinguishable passes alike:
+ *   photonic_engines/clifford/sampler.py:391-460          _sample_streams (the step loop)
+ *   photonic_engines/clifford/cofactors_triton.py:413-485 multiplicity_tables, plan_multi,
+ *                                                          cofactor_partials_multi
+ *   photonic_engines/clifford/cuda_cofactors.py:278-299   cofactor_partials_cuda (cof_multi)
+ *   photonic_engines/clifford/cofactors_triton.py:533-545 draw_step (_draw_kernel)
+ *
+ * precision: PE_PRECISION_F64 or PE_PRECISION_MIXED.  block_threads: 64, 128 or 256 (0 = default).
+ * tpl: threads per Gray lane (1, 2 or 4; 0 = default).  grid_ctas: persistent CTAs (0 = occupancy).
+ */
+int pe_fock_chain(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
+                  const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
+                  const int32_t* d_nk, const int64_t* d_cols, int n_stride, const double* d_uniforms,
+                  const int64_t* d_seeds, const int64_t* d_seed_row, const int64_t* d_rng_off,
+                  const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
+                  int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
+                  int grid_ctas, void* stream);
+
+/*
+ * Laplace cofactors P[s, c] = per(A_s[rows_s, all columns but c]) of S blocks, the reference's
+ * 2020 kernel entry point:
+ *   photonic_engines/clifford/cofactors_triton.py:509-530  laplace_cofactors_rows
+ * d_a: complex128 [S][m][K] (interleaved), d_rows int64 [S][K - 1] (repeats allowed, < m),
+ * d_p: complex128 [S][K] out.  K <= PE_MAX_PHOTONS.
+ */
+int pe_cofactors_rows(int precision, const double* d_a, const int64_t* d_rows, int64_t S, int m, int K,
+                      double* d_p, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
+                      void* stream);
+
+/* Arithmetic-pipe probe (no counterpart in the reference: a measurement aid).  Launches 8 independent
+ * FMA chains per thread, `iters` rounds, on (SMs x 8) CTAs of 256 threads, in FP64
+ * (PE_PRECISION_F64) or FP32 (PE_PRECISION_MIXED); *flops receives the FLOPs the launch performs
+ * (FMA = 2).  d_out needs SMs * 8 * 256 * sizeof(element) bytes.  The caller times it. */
+int pe_pipe_probe(int precision, int iters, void* d_out, size_t out_bytes, double* flops, void* stream);
+
+/* Copy the device status word of a workspace to *status (synchronises `stream`).
+ * 0 = no device-side error; otherwise PE_ERR_DEVICE and the offending stream index in *detail. */
+int pe_read_status(const void* d_workspace, int* status, int64_t* detail, void* stream);
+
+/* Human-readable text of a status code. */
+const char* pe_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PE_B200_H */

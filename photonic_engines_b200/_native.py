@@ -1,0 +1,118 @@
+"""ctypes binding of the CUDA library `libpe_b200.so` (C ABI declared in include/pe_b200.h).
+
+The library is the only compute path: when it is missing, or no CUDA device is visible, every
+sampling call raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpe_b200.so")
+
+PE_OK = 0
+PE_PRECISION_F64 = 0
+PE_PRECISION_MIXED = 1
+PE_MAX_PHOTONS = 32
+PRECISIONS = {"f64": PE_PRECISION_F64, "mixed": PE_PRECISION_MIXED}
+
+_lib = None
+_vp = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_i32 = ctypes.c_int
+
+
+class NativeError(RuntimeError):
+    """A status < 0 returned by the CUDA library, or the library missing."""
+
+
+def load() -> ctypes.CDLL:
+    """Load libpe_b200.so (raises NativeError when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise NativeError(f"{LIB_PATH} is missing: build it with `python -m photonic_engines_b200.build` "
+                          "(there is no non-CUDA path)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.pe_version.restype = _i32
+    L.pe_version.argtypes = []
+    L.pe_max_modes.restype = _i32
+    L.pe_max_modes.argtypes = [_i32]
+    L.pe_chain_workspace_bytes.restype = ctypes.c_size_t
+    L.pe_chain_workspace_bytes.argtypes = [_i64]
+    L.pe_fock_chain.restype = _i32
+    L.pe_fock_chain.argtypes = [_i32, _vp, _vp, _vp, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp,
+                                _vp, _vp, _vp, _i32, _vp, _i32, _vp, ctypes.c_size_t, _i32, _i32, _i32, _vp]
+    L.pe_cofactors_rows.restype = _i32
+    L.pe_cofactors_rows.argtypes = [_i32, _vp, _vp, _i64, _i32, _i32, _vp, _vp, ctypes.c_size_t, _i32, _i32, _vp]
+    L.pe_pipe_probe.restype = _i32
+    L.pe_pipe_probe.argtypes = [_i32, _i32, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double), _vp]
+    L.pe_read_status.restype = _i32
+    L.pe_read_status.argtypes = [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i64), _vp]
+    L.pe_status_string.restype = ctypes.c_char_p
+    L.pe_status_string.argtypes = [_i32]
+    _lib = L
+    return L
+
+
+# every symbol the C header declares (checked by the CPU test that loads the library)
+EXPORTED = ("pe_version", "pe_max_modes", "pe_chain_workspace_bytes", "pe_fock_chain", "pe_cofactors_rows",
+            "pe_pipe_probe", "pe_read_status", "pe_status_string")
+
+
+def check(rc: int, what: str) -> None:
+    if rc != PE_OK:
+        msg = load().pe_status_string(rc).decode()
+        raise NativeError(f"{what}: status {rc} ({msg})")
+
+
+def ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def stream_handle(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def require_cuda(t: torch.Tensor, name: str) -> None:
+    if not torch.cuda.is_available():
+        raise NativeError("no CUDA device is visible: the B200 sampler has no CPU path")
+    if t.device.type != "cuda":
+        raise ValueError(f"{name} must be a CUDA tensor (got {t.device})")
+
+
+def workspace(device: torch.device) -> torch.Tensor:
+    """A fresh device workspace for one call (queue counter + status word)."""
+    n = int(load().pe_chain_workspace_bytes(0))
+    return torch.empty(n, dtype=torch.uint8, device=device)
+
+
+def read_status(ws: torch.Tensor) -> tuple[int, int]:
+    st = _i32(0)
+    det = _i64(0)
+    check(load().pe_read_status(ptr(ws), ctypes.byref(st), ctypes.byref(det), stream_handle(ws.device)),
+          "pe_read_status")
+    return int(st.value), int(det.value)
+
+
+def pipe_peak_tflops(precision: str, device, iters: int = 4096, reps: int = 5) -> float:
+    """Measured FP64 ("f64") or FP32 ("mixed") FMA-pipe peak of the device, TFLOP/s (best of `reps`)."""
+    L = load()
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    out = torch.empty(sms * 8 * 256, dtype=torch.float64, device=device)
+    fl = ctypes.c_double(0.0)
+    best = 0.0
+    s = stream_handle(out.device)
+    for _ in range(reps + 1):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        check(L.pe_pipe_probe(PRECISIONS[precision], iters, ptr(out), out.numel() * 8, ctypes.byref(fl), s),
+              "pe_pipe_probe")
+        e1.record()
+        e1.synchronize()
+        best = max(best, fl.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best

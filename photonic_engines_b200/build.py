@@ -1,0 +1,72 @@
+"""Build of the CUDA library `libpe_b200.so` (in-tree, next to this file) for sm_100a.
+
+Every kernel variant (precision x threads per Gray lane x largest column tier) is one object file
+compiled from csrc/fock_inst.cu with its own -D flags, in parallel; csrc/fock_api.cu holds the C ABI.
+Objects are rebuilt only when a source is newer.  `python -m photonic_engines_b200.build` builds it.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libpe_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+
+# (mixed, threads per lane, largest tier) of every compiled chain/cofactor kernel pair
+VARIANTS = [(mx, tpl, kpm) for mx in (0, 1) for tpl, kpms in ((1, (8, 16)), (2, (8, 16, 20, 24, 28, 32)),
+                                                              (4, (8, 16, 20, 24, 28, 32))) for kpm in kpms]
+
+
+def _sources():
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))] + \
+        [os.path.join(ROOT, "include", "pe_b200.h"), os.path.abspath(__file__)]
+
+
+def _stale(target: str, deps) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return r.stdout + r.stderr
+
+
+def build(jobs: int | None = None, verbose: bool = False, ptxas_info: bool = False) -> str:
+    """Compile every variant and link the library; returns its path."""
+    os.makedirs(OBJ, exist_ok=True)
+    deps = _sources()
+    tasks = []
+    for mx, tpl, kpm in VARIANTS:
+        obj = os.path.join(OBJ, f"fock_m{mx}_t{tpl}_k{kpm}.o")
+        if _stale(obj, deps):
+            tasks.append([NVCC, *ARCH, *FLAGS, *(["-Xptxas", "-v"] if ptxas_info else []), f"-DPE_MIXED={mx}",
+                          f"-DPE_TPL={tpl}", f"-DPE_KPM={kpm}", "-c", os.path.join(CSRC, "fock_inst.cu"), "-o", obj])
+    api_obj = os.path.join(OBJ, "fock_api.o")
+    if _stale(api_obj, deps):
+        tasks.append([NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, "fock_api.cu"), "-o", api_obj])
+    objs = [os.path.join(OBJ, f"fock_m{mx}_t{tpl}_k{kpm}.o") for mx, tpl, kpm in VARIANTS] + [api_obj]
+    if tasks:
+        with ThreadPoolExecutor(jobs or os.cpu_count() or 4) as ex:
+            for out in ex.map(_run, tasks):
+                if verbose and out.strip():
+                    print(out)
+    if tasks or _stale(LIB, objs):
+        _run([NVCC, *ARCH, "-shared", "-o", LIB, *objs])
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, ptxas_info="--ptxas" in sys.argv))

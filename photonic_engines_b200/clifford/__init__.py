@@ -1,0 +1,26 @@
+"""Exact Clifford & Clifford Fock sampler on B200 (arXiv:1706.01260, arXiv:2005.04214).
+
+    fock_sample(U, in_modes, shots, generator, loss=, indist=, ...)   the reference's entry point
+    sample(FockState, U, shots, generator, ...)                        dispatch on the input state
+    sample_chains(U, in_modes, sigma, uniforms=...)                     chains with a given column order
+    laplace_cofactors_rows(A, rows)                                     the cofactor step alone
+
+Mirrors photonic_engines/clifford/__init__.py:139-166 for Fock inputs; other input types (emitter,
+superposition) are not part of this library and raise.
+"""
+from __future__ import annotations
+
+import torch
+
+from ..states import FockState
+from .kernels import laplace_cofactors_rows
+from .sampler import fock_sample, sample_chains
+
+__all__ = ["fock_sample", "laplace_cofactors_rows", "sample", "sample_chains"]
+
+
+def sample(state, U: torch.Tensor, shots: int, generator: torch.Generator | None = None, **kw):
+    """Exact samples [shots, m] for a FockState input (`fock_sample` on its modes)."""
+    if isinstance(state, FockState):
+        return fock_sample(U, state.modes(), shots, generator=generator, **kw)
+    raise TypeError(f"unsupported input state {type(state).__name__}: this library samples Fock inputs only")

@@ -1,0 +1,129 @@
+"""Typed torch-side wrappers of the two compute entry points of the CUDA library.
+
+    chain(...)                 pe_fock_chain: whole Clifford & Clifford chains in one persistent launch
+    laplace_cofactors_rows(..) pe_cofactors_rows: the cofactor step alone
+                               (photonic_engines/clifford/cofactors_triton.py:509-530)
+    pack_instances(...)        circuit input columns -> the column-major instance layout the chain reads
+
+All tensors are CUDA tensors; launches go on torch's current stream of that device.
+"""
+from __future__ import annotations
+
+import torch
+
+from .. import _native as N
+
+
+def pack_instances(U: torch.Tensor, in_modes) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor]:
+    """U [B, m, m] (or [m, m]) and the n input modes -> (acol, inst_off, inst_m, inst_n).
+
+    Instance b holds the n input columns U[b][:, in_modes] column-major: acol[b, j, rho] = U[b, rho, in_modes[j]],
+    complex128, so that one input column is m contiguous complex values.
+    """
+    if U.dim() == 2:
+        U = U[None]
+    B, m, _ = U.shape
+    idx = torch.as_tensor(list(in_modes), dtype=torch.int64, device=U.device)
+    acol = U.to(torch.complex128)[:, :, idx].transpose(1, 2).contiguous()            # [B, n, m]
+    n = idx.shape[0]
+    dev = U.device
+    inst_off = torch.arange(B, dtype=torch.int64, device=dev) * (n * m)
+    inst_m = torch.full((B,), m, dtype=torch.int32, device=dev)
+    inst_n = torch.full((B,), n, dtype=torch.int32, device=dev)
+    return acol, inst_off, inst_m, inst_n
+
+
+def pack_ragged(circuits) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor]:
+    """Instances of different sizes: circuits = [(U_g [m_g, m_g], in_modes_g)] -> one flat acol buffer with
+    per-instance offsets, modes and column counts (the many-instance batch)."""
+    parts, off, ms, ns = [], [], [], []
+    pos = 0
+    dev = circuits[0][0].device
+    for U, modes in circuits:
+        idx = torch.as_tensor(list(modes), dtype=torch.int64, device=U.device)
+        a = U.to(torch.complex128)[:, idx].transpose(0, 1).contiguous().reshape(-1)   # [n_g * m_g]
+        parts.append(a)
+        off.append(pos)
+        ms.append(U.shape[0])
+        ns.append(idx.shape[0])
+        pos += a.shape[0]
+    acol = torch.cat(parts)
+    return (acol, torch.tensor(off, dtype=torch.int64, device=dev), torch.tensor(ms, dtype=torch.int32, device=dev),
+            torch.tensor(ns, dtype=torch.int32, device=dev))
+
+
+def _i64(t, dev):
+    return None if t is None else torch.as_tensor(t, dtype=torch.int64, device=dev).contiguous()
+
+
+def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst_n: torch.Tensor, dp, cols, *,
+          m_max: int | None = None, nk=None, uniforms=None, seeds=None, seed_row=None, rng_off=None, order=None,
+          want_occ: bool = True, occ_stride: int | None = None, want_marg: bool = False, precision: str = "f64",
+          block_threads: int = 0, tpl: int = 0, grid_ctas: int = 0, check_status: bool = True, out=None):
+    """Run the chains of S streams.  dp [S] instance per stream, cols [S, n_stride] input columns in chain order,
+    nk [S] photons per stream (None: n_stride), uniforms [S, n_stride] (None: Philox from seeds [R, n_stride],
+    seed_row [S], rng_off [S]).  Returns (rows [S, n_stride] int64, occ [S, occ_stride] or None,
+    marg [S, n_stride, m_max] or None).  `out` may hold preallocated (rows, occ, marg) tensors."""
+    N.require_cuda(acol, "acol")
+    dev = acol.device
+    L = N.load()
+    if precision not in N.PRECISIONS:
+        raise ValueError(f"unknown precision {precision!r}: 'f64' or 'mixed'")
+    dp = _i64(dp, dev)
+    cols = _i64(cols, dev)
+    S, n_stride = cols.shape
+    if n_stride > N.PE_MAX_PHOTONS:
+        raise ValueError(f"at most {N.PE_MAX_PHOTONS} photons per stream (got {n_stride})")
+    if m_max is None:
+        m_max = int(inst_m.max().item())
+    occ_stride = occ_stride or m_max
+    nk_t = None if nk is None else torch.as_tensor(nk, dtype=torch.int32, device=dev).contiguous()
+    u_t = None if uniforms is None else torch.as_tensor(uniforms, dtype=torch.float64, device=dev).contiguous()
+    seeds_t = _i64(seeds, dev)
+    if u_t is None and seeds_t is None:
+        raise ValueError("either uniforms or seeds")
+    if seeds_t is not None and seeds_t.dim() == 1:
+        seeds_t = seeds_t[None]
+    if seeds_t is not None and seeds_t.shape[-1] != n_stride:
+        seeds_t = torch.nn.functional.pad(seeds_t, (0, n_stride - seeds_t.shape[-1])).contiguous()
+    if out is not None:
+        rows, occ, marg = out
+    else:
+        rows = torch.zeros(S, n_stride, dtype=torch.int64, device=dev)
+        occ = torch.empty(S, occ_stride, dtype=torch.int64, device=dev) if want_occ else None
+        marg = torch.zeros(S, n_stride, m_max, dtype=torch.float64, device=dev) if want_marg else None
+    ws = N.workspace(dev)
+    a = acol if acol.dtype == torch.float64 else torch.view_as_real(acol.contiguous())
+    rc = L.pe_fock_chain(N.PRECISIONS[precision], N.ptr(a), N.ptr(inst_off), N.ptr(inst_m), N.ptr(inst_n),
+                         int(inst_off.shape[0]), int(m_max), int(S), N.ptr(dp), N.ptr(nk_t), N.ptr(cols), int(n_stride),
+                         N.ptr(u_t), N.ptr(seeds_t), N.ptr(_i64(seed_row, dev)), N.ptr(_i64(rng_off, dev)),
+                         N.ptr(_i64(order, dev)), N.ptr(rows), N.ptr(occ), int(occ_stride), N.ptr(marg),
+                         int(m_max), N.ptr(ws), int(ws.numel()), int(block_threads), int(tpl), int(grid_ctas),
+                         N.stream_handle(dev))
+    N.check(rc, "pe_fock_chain")
+    if check_status:
+        st, det = N.read_status(ws)
+        if st != 0:
+            raise N.NativeError(f"pe_fock_chain: device-side index error at stream {det} (status {st})")
+    return rows, occ, marg
+
+
+def laplace_cofactors_rows(A: torch.Tensor, rows: torch.Tensor, precision: str = "f64", block_threads: int = 0,
+                           tpl: int = 0) -> torch.Tensor:
+    """P [S, K] with P[s, c] = per(A[s][rows[s]] without column c); A [S, m, K] complex128, rows [S, K - 1]
+    (repeats allowed).  Same contract as the reference's laplace_cofactors_rows."""
+    N.require_cuda(A, "A")
+    S, m, K = A.shape
+    dev = A.device
+    A2 = torch.view_as_real(A.to(torch.complex128).contiguous())
+    rows = torch.as_tensor(rows, dtype=torch.int64, device=dev).reshape(S, K - 1).contiguous()
+    P = torch.empty(S, K, dtype=torch.complex128, device=dev)
+    ws = N.workspace(dev)
+    rc = N.load().pe_cofactors_rows(N.PRECISIONS[precision], N.ptr(A2), N.ptr(rows) if K > 1 else None, int(S), int(m),
+                                    int(K), N.ptr(torch.view_as_real(P)), N.ptr(ws), int(ws.numel()), int(block_threads),
+                                    int(tpl), N.stream_handle(dev))
+    N.check(rc, "pe_cofactors_rows")
+    st, det = N.read_status(ws)
+    if st != 0:
+        raise N.NativeError(f"pe_cofactors_rows: device-side index error at block {det}")
+    return P

@@ -1,0 +1,225 @@
+// C ABI of the Fock chain kernels (declared in include/pe_b200.h): argument checks, variant
+// lookup, occupancy-sized persistent grid, workspace reset, launch on the caller's stream.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fock_kernels.cuh"
+#include "fock_registry.h"
+
+namespace pe {
+
+constexpr int N_KPM = 6;
+constexpr int KPM_LADDER[N_KPM] = {8, 16, 20, 24, 28, 32};
+static int kpm_for(int n) {
+    for (int i = 0; i < N_KPM; ++i) if (n <= KPM_LADDER[i]) return KPM_LADDER[i];
+    return -1;
+}
+static int tpl_index(int tpl) { return tpl == 1 ? 0 : tpl == 2 ? 1 : tpl == 4 ? 2 : -1; }
+static int kpm_index(int kpm) {
+    for (int i = 0; i < N_KPM; ++i) if (KPM_LADDER[i] == kpm) return i;
+    return -1;
+}
+
+static void* g_chain[2][3][N_KPM];
+static void* g_cof[2][3][N_KPM];
+
+void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cofactor_kernel) {
+    const int ti = tpl_index(tpl), ki = kpm_index(kpm);
+    if (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) return;
+    g_chain[mixed][ti][ki] = chain_kernel;
+    g_cof[mixed][ti][ki] = cofactor_kernel;
+}
+void* find_chain_kernel(int mixed, int tpl, int kpm) {
+    const int ti = tpl_index(tpl), ki = kpm_index(kpm);
+    return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_chain[mixed][ti][ki];
+}
+void* find_cofactor_kernel(int mixed, int tpl, int kpm) {
+    const int ti = tpl_index(tpl), ki = kpm_index(kpm);
+    return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_cof[mixed][ti][ki];
+}
+
+static int default_tpl(int kpm) { return kpm <= 8 ? 1 : (kpm <= 24 ? 2 : 4); }
+
+static int max_smem_optin() {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+    return v;
+}
+
+// Arithmetic-pipe probe: 8 independent FMA chains per thread, `iters` rounds.  Used by the benchmark to
+// measure the FP64 / FP32 peak of the GPU it runs on (the roofline denominator of the chain kernels).
+template <typename T>
+__global__ void pipe_probe_kernel(T* out, T a, T b, int iters) {
+    T x[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) x[i] = (T)(threadIdx.x + i);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = x[i] * a + b;
+    }
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += x[i];
+    out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace pe
+
+using namespace pe;
+
+extern "C" int pe_version(void) { return 100; }
+
+extern "C" int pe_max_modes(int block_threads) {
+    (void)block_threads;
+    const int cap = max_smem_optin();
+    if (cap <= 0) return 0;
+    return (int)((cap - (int)smem_fixed_bytes()) / (int)sizeof(double));
+}
+
+extern "C" size_t pe_chain_workspace_bytes(int64_t S) {
+    (void)S;
+    return WS_BYTES;
+}
+
+extern "C" const char* pe_status_string(int status) {
+    switch (status) {
+        case PE_OK: return "ok";
+        case PE_ERR_ARG: return "invalid argument (null pointer, negative size or unknown option)";
+        case PE_ERR_SIZE: return "size beyond the compiled limits (photons, modes or workspace)";
+        case PE_ERR_CUDA: return "CUDA runtime error at launch";
+        case PE_ERR_DEVICE: return "index out of range found on the device";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int pe_read_status(const void* d_workspace, int* status, int64_t* detail, void* stream) {
+    if (!d_workspace || !status) return PE_ERR_ARG;
+    int st = 0;
+    long long det = 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemcpyAsync(&st, (const char*)d_workspace + 8, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PE_ERR_CUDA;
+    if (cudaMemcpyAsync(&det, (const char*)d_workspace + 16, sizeof(long long), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PE_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PE_ERR_CUDA;
+    *status = st;
+    if (detail) *detail = (int64_t)det;
+    return PE_OK;
+}
+
+static int launch_prepare(void* fn, int block, size_t smem, int* grid_per_sm) {
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return PE_ERR_CUDA;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, smem) != cudaSuccess) return PE_ERR_CUDA;
+    if (occ < 1) return PE_ERR_SIZE;
+    *grid_per_sm = occ;
+    return PE_OK;
+}
+
+extern "C" int pe_fock_chain(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
+                             const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
+                             const int32_t* d_nk, const int64_t* d_cols, int n_stride, const double* d_uniforms,
+                             const int64_t* d_seeds, const int64_t* d_seed_row, const int64_t* d_rng_off,
+                             const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
+                             int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
+                             int grid_ctas, void* stream) {
+    if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
+    if (S < 0 || G < 1 || m_max < 1 || n_stride < 1) return PE_ERR_ARG;
+    if (!d_acol || !d_inst_off || !d_inst_m || !d_inst_n || !d_dp || !d_cols || !d_rows || !d_workspace) return PE_ERR_ARG;
+    if (!d_uniforms && !d_seeds) return PE_ERR_ARG;
+    if (d_occ && occ_stride < m_max) return PE_ERR_ARG;
+    if (d_marg && marg_stride < m_max) return PE_ERR_ARG;
+    if (workspace_bytes < WS_BYTES || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
+    const int kpm = kpm_for(n_stride);
+    if (kpm < 0) return PE_ERR_SIZE;
+    if (tpl == 0) tpl = default_tpl(kpm);
+    if (tpl_index(tpl) < 0) return PE_ERR_ARG;
+    void* fn = find_chain_kernel(precision, tpl, kpm);
+    if (!fn) return PE_ERR_SIZE;
+    const int block = block_threads ? block_threads : 256;
+    if (block < 32 || block > 256 || (block & 31) || block < 32 * 1) return PE_ERR_ARG;
+    const size_t smem = smem_fixed_bytes() + (size_t)m_max * sizeof(double);
+    const int cap = max_smem_optin();
+    if (cap <= 0) return PE_ERR_CUDA;
+    if (smem > (size_t)cap) return PE_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(d_workspace, 0, WS_BYTES, st) != cudaSuccess) return PE_ERR_CUDA;
+    if (S == 0) return PE_OK;
+    int per_sm = 0;
+    int rc = launch_prepare(fn, block, smem, &per_sm);
+    if (rc != PE_OK) return rc;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int64_t grid = grid_ctas > 0 ? grid_ctas : (int64_t)sms * per_sm;
+    if (grid > S) grid = S;
+    if (grid < 1) grid = 1;
+    ChainParams p;
+    p.acol = (const double2*)d_acol;
+    p.inst_off = d_inst_off; p.inst_m = d_inst_m; p.inst_n = d_inst_n; p.G = G;
+    p.S = S; p.dp = d_dp; p.nk = d_nk; p.cols = d_cols; p.n_stride = n_stride;
+    p.uniforms = d_uniforms; p.seeds = d_seeds; p.seed_row = d_seed_row; p.rng_off = d_rng_off; p.order = d_order;
+    p.rows = d_rows; p.occ = d_occ; p.occ_stride = d_occ ? occ_stride : m_max; p.marg = d_marg; p.marg_stride = marg_stride;
+    p.queue = (unsigned long long*)d_workspace;
+    p.status = (int*)((char*)d_workspace + 8);
+    p.detail = (long long*)((char*)d_workspace + 16);
+    p.m_cap = m_max;
+    p.tau = 2.0e-6;
+    void* args[] = {&p};
+    if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st) != cudaSuccess) return PE_ERR_CUDA;
+    return PE_OK;
+}
+
+extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t* d_rows, int64_t S, int m, int K,
+                                 double* d_p, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
+                                 void* stream) {
+    if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
+    if (S < 0 || m < 1 || K < 1 || !d_a || !d_p || !d_workspace) return PE_ERR_ARG;
+    if (K > 1 && !d_rows) return PE_ERR_ARG;
+    if (workspace_bytes < WS_BYTES || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
+    const int kpm = kpm_for(K);
+    if (kpm < 0) return PE_ERR_SIZE;
+    if (tpl == 0) tpl = default_tpl(kpm);
+    if (tpl_index(tpl) < 0) return PE_ERR_ARG;
+    void* fn = find_cofactor_kernel(precision, tpl, kpm);
+    if (!fn) return PE_ERR_SIZE;
+    const int block = block_threads ? block_threads : 256;
+    if (block < 32 || block > 256 || (block & 31)) return PE_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(d_workspace, 0, WS_BYTES, st) != cudaSuccess) return PE_ERR_CUDA;
+    if (S == 0) return PE_OK;
+    const size_t smem = smem_fixed_bytes();
+    int per_sm = 0;
+    int rc = launch_prepare(fn, block, smem, &per_sm);
+    if (rc != PE_OK) return rc;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int64_t grid = (int64_t)sms * per_sm;
+    if (grid > S) grid = S;
+    const double2* a = (const double2*)d_a;
+    double2* pp = (double2*)d_p;
+    int* status = (int*)((char*)d_workspace + 8);
+    long long* detail = (long long*)((char*)d_workspace + 16);
+    void* args[] = {(void*)&a, (void*)&d_rows, (void*)&S, (void*)&m, (void*)&K, (void*)&pp, (void*)&status, (void*)&detail};
+    if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st) != cudaSuccess) return PE_ERR_CUDA;
+    return PE_OK;
+}
+
+extern "C" int pe_pipe_probe(int precision, int iters, void* d_out, size_t out_bytes, double* flops, void* stream) {
+    if ((precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) || iters < 1 || !d_out || !flops)
+        return PE_ERR_ARG;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PE_ERR_CUDA;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return PE_ERR_CUDA;
+    const int threads = 256, blocks = sms * 8;
+    const size_t need = (size_t)blocks * threads * (precision == PE_PRECISION_F64 ? 8 : 4);
+    if (out_bytes < need) return PE_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (precision == PE_PRECISION_F64)
+        pipe_probe_kernel<double><<<blocks, threads, 0, st>>>((double*)d_out, 0.999999, 1e-7, iters);
+    else
+        pipe_probe_kernel<float><<<blocks, threads, 0, st>>>((float*)d_out, 0.999999f, 1e-7f, iters);
+    if (cudaGetLastError() != cudaSuccess) return PE_ERR_CUDA;
+    *flops = 2.0 * 8.0 * (double)iters * (double)blocks * (double)threads;
+    return PE_OK;
+}

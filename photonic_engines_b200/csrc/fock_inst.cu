@@ -1,0 +1,20 @@
+// One kernel variant, selected at compile time: PE_MIXED (0 / 1), PE_TPL (threads per Gray lane)
+// and PE_KPM (largest cofactor tier the chain kernel contains).  The build compiles this file once
+// per variant, in parallel, and links the objects into one library.
+#include "fock_kernels.cuh"
+#include "fock_registry.h"
+
+#if !defined(PE_MIXED) || !defined(PE_TPL) || !defined(PE_KPM)
+#error "PE_MIXED, PE_TPL and PE_KPM must be defined"
+#endif
+
+namespace {
+struct Registration {
+    Registration() {
+        pe::register_variant(PE_MIXED, PE_TPL, PE_KPM,
+                             (void*)pe::fock_chain_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
+                             (void*)pe::cofactor_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>);
+    }
+};
+Registration registration;
+}  // namespace

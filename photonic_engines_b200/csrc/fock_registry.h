@@ -1,0 +1,11 @@
+// Registry of the compiled kernel variants (precision x threads-per-lane x largest column tier).
+// Every variant object file registers its two kernels at load time; the C ABI looks them up.
+#pragma once
+
+namespace pe {
+
+void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cofactor_kernel);
+void* find_chain_kernel(int mixed, int tpl, int kpm);
+void* find_cofactor_kernel(int mixed, int tpl, int kpm);
+
+}  // namespace pe

@@ -1,0 +1,96 @@
+// Device building blocks of the Fock chain kernels: Philox uniforms, exact signed binomials, complex
+// helpers and the per-CTA shared-memory layout.  sm_100a only.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pe {
+
+constexpr int MAXN = 32;        // photons per stream = largest cofactor tier (columns)
+constexpr int LIN_MAX = 512;    // inner Gray block: terms enumerated from the shared schedule table
+constexpr int MAX_WARPS = 8;    // CTA of at most 256 threads
+
+// ------------------------------------------------------------------------------------------ RNG
+// Philox4x32-10 with the counter/key arrangement of Triton's tl.rand for an int32 offset and a
+// seed below 2^31 (triton/language/random.py: randint4x -> philox -> philox_impl): counter
+// (offset, 0, 0, 0), key (seed_lo, seed_hi), first output word.
+static __device__ __forceinline__ uint32_t philox_word0(uint64_t seed, uint32_t offset) {
+    uint32_t c0 = offset, c1 = 0u, c2 = 0u, c3 = 0u;
+    uint32_t k0 = (uint32_t)(seed & 0xffffffffull), k1 = (uint32_t)(seed >> 32);
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t o0 = c0, o2 = c2;
+        c0 = __umulhi(0xCD9E8D57u, o2) ^ c1 ^ k0;
+        c2 = __umulhi(0xD2511F53u, o0) ^ c3 ^ k1;
+        c1 = 0xCD9E8D57u * o2;
+        c3 = 0xD2511F53u * o0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c0;
+}
+
+// tl.rand: the word as int32, negatives folded to -x - 1, times float32(4.6566127342e-10), in f32.
+static __device__ __forceinline__ float triton_uniform_f32(uint64_t seed, uint32_t offset) {
+    int32_t x = (int32_t)philox_word0(seed, offset);
+    if (x < 0) x = -x - 1;
+    return __fmul_rn(__int2float_rn(x), 4.6566127342e-10f);
+}
+
+// The draw kernel's 48-bit uniform of stream-offset `off`: (r0 + r1 2^-24) / (1 + 2^-24), f64.
+static __device__ __forceinline__ double chain_uniform(uint64_t seed, int64_t off) {
+    const double r0 = (double)triton_uniform_f32(seed, (uint32_t)(2 * off));
+    const double r1 = (double)triton_uniform_f32(seed, (uint32_t)(2 * off + 1));
+    const double num = __dadd_rn(r0, __dmul_rn(r1, 5.9604644775390625e-08));
+    return __ddiv_rn(num, 1.0 + 5.9604644775390625e-08);
+}
+
+// ------------------------------------------------------------------------------------------ maths
+// (-1)^v C(M, v), exact: the integer product is formed in int64 (M <= 32) before conversion.
+static __device__ __forceinline__ double signed_binom(int M, int v) {
+    int64_t c = 1;
+    for (int i = 0; i < v; ++i) c = c * (M - i) / (i + 1);
+    return (v & 1) ? -(double)c : (double)c;
+}
+
+// ------------------------------------------------------------------------------------------ layout
+// Per-step plan of one stream, written by thread 0.  Kernel digits are ordered
+//   [inner: nin | middle: nmid | high: nhi | fixed: nfix]
+// inner digits are walked from the shared schedule table (one CTA-uniform transition per term),
+// middle digits by an odometer once per inner block, high digits index the Gray lanes, fixed
+// digits have radix 1 (their sign never changes).
+struct Plan {
+    int64_t N;          // terms of the collapsed sum (the reference's addend count)
+    int64_t H;          // lanes = product of high radices
+    int64_t Lmid;       // middle combinations per lane
+    int Lin;            // inner combinations per block (<= LIN_MAX)
+    int K, K1, D;       // columns, chosen rows, digits (distinct chosen rows)
+    int nin, nmid, nhi;
+    double scale;       // 2^-K1, doubled when the top digit is halved
+    int R[MAXN];        // radix per kernel digit
+    int M[MAXN];        // multiplicity per kernel digit
+    int drow[MAXN];     // output mode per kernel digit
+    unsigned char vend[MAXN];   // inner digit values after a forward inner block
+};
+
+struct Smem {
+    Plan plan;
+    double2 P[MAXN];               // cofactors of the step (scaled)
+    double2 B[MAXN][MAXN];         // B[kd][j] = A[drow_kd, col_j], padded columns zero
+    float2 B32[MAXN][MAXN];        // 2 * B in float32 (the mixed form's Gray update)
+    double tab_w[LIN_MAX];         // inner weight prod (-1)^v C(M, v) at inner index t
+    float tab_w32[LIN_MAX];
+    unsigned char tab_f[LIN_MAX];  // transition into t: digit | 0x80 when the update is -2 b
+    double2 red[MAX_WARPS][MAXN];  // cross-warp reduction
+    double scan[MAX_WARPS];
+    double fmin[MAX_WARPS];
+    int cnt[MAX_WARPS];
+    int rows[MAXN];                // chosen modes so far
+    int cols[MAXN];                // input columns of the stream in chain order
+    int64_t cur;                   // stream being processed (-1: queue drained)
+    double tot, target, u;
+    int bad;                       // set by any thread that saw an out-of-range index
+    int refine;                    // mixed form: the draw fell inside the guard band
+};
+
+}  // namespace pe

@@ -1,0 +1,196 @@
+"""Generate the golden fixtures of the Fock sampling path from the REFERENCE implementation itself.
+
+Run in a container where the reference project is importable (it is NOT needed at test time):
+
+    python tests/golden/make_golden.py /path/to/photonic-engines
+
+It imports the reference read-only and records, with CPU tensors and the Triton CPU interpreter:
+
+  philox.npz   tl.rand(seed, offset) bit patterns and the draw kernel's 48-bit uniforms, from a
+               Triton kernel written here that calls tl.rand exactly as the reference's draw kernel
+               does (photonic_engines/clifford/cofactors_triton.py:303-305).
+  steps.npz    cofactors of blocks with repeated rows (variants.cofactors_2020, variants.py:96-114),
+               the reference's extended-precision emulation of its kernel code
+               (cuda_rect.rect_cofactors_emul, real="long double", form="fock", cuda_rect.py:959-985),
+               and step amplitudes (variants.step_amplitudes, variants.py:176-194) on the
+               reference's own test steps (tests/clifford/test_variants.py:41-49).
+  chains.npz   whole chains drawn by the reference's sampler: `_sample_streams`
+               (sampler.py:391-460) rows [S, n] in chain order, plus the sigma and per-step seeds
+               the generator produced, and `fock_sample` occupations with loss / partial
+               distinguishability (sampler.py:183-215) for a seeded CPU generator.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+os.environ["TRITON_INTERPRET"] = "1"          # the reference's Triton kernels run on the CPU interpreter
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def haar(m: int, seed: int) -> torch.Tensor:
+    """tests/helpers.py:10-17 of the reference (seeded QR of a complex Gaussian, phases fixed)."""
+    g = torch.Generator().manual_seed(seed)
+    z = torch.randn(m, m, generator=g, dtype=torch.float64) + 1j * torch.randn(m, m, generator=g, dtype=torch.float64)
+    q, r = torch.linalg.qr(z)
+    d = torch.diagonal(r)
+    return q * (d / d.abs()).unsqueeze(0)
+
+
+def make_philox():
+    import triton
+    import triton.language as tl
+
+    @triton.jit
+    def rand_kernel(out_ptr, seed, N: tl.constexpr):
+        s = tl.arange(0, N)
+        tl.store(out_ptr + s, tl.rand(seed, s))
+
+    @triton.jit(do_not_specialize=["seed"])
+    def uniform_kernel(out_ptr, seed):
+        s = tl.program_id(0)
+        two = tl.arange(0, 2)
+        r = tl.rand(seed, s * 2 + two).to(tl.float64)
+        u = tl.sum(tl.where(two == 0, r, r * 5.9604644775390625e-08), axis=0) / (1.0 + 5.9604644775390625e-08)
+        tl.store(out_ptr + s, u)
+
+    seeds = np.array([0, 1, 7, 12345, 2 ** 31 - 2, 987654321, 1804289383], dtype=np.int64)
+    rand_bits = np.zeros((len(seeds), 128), dtype=np.uint32)
+    unif = np.zeros((len(seeds), 96), dtype=np.float64)
+    for i, sd in enumerate(seeds.tolist()):
+        out = torch.zeros(128, dtype=torch.float32)
+        rand_kernel[(1,)](out, sd, N=128)
+        rand_bits[i] = out.numpy().view(np.uint32)
+        u = torch.zeros(96, dtype=torch.float64)
+        uniform_kernel[(96,)](u, sd)
+        unif[i] = u.numpy()
+    np.savez_compressed(os.path.join(HERE, "philox.npz"), seeds=seeds, rand_bits=rand_bits, uniforms=unif)
+
+
+# the reference's own step cases (tests/clifford/test_variants.py:41-49) and collision patterns
+# (tests/clifford/check_multi.py:22-30)
+STEPS = [
+    ([], [3]),
+    ([4], [0, 0]),
+    ([1, 1, 1], [2, 2, 0, 0]),
+    ([0, 2, 2, 5], [0, 1, 1, 2, 3]),
+    ([0, 1, 2, 3], [0, 1, 2, 3, 4]),
+    ([2, 2, 2, 2], [0, 0, 0, 0, 1]),
+    ([3, 3, 1, 0, 6, 6], [0, 1, 2, 3, 4, 5, 6]),
+]
+PATTERNS = [
+    [0], [0, 0], [0, 1], [0, 0, 0], [1, 1, 0], [2, 1, 0], [0, 0, 0, 0], [1, 1, 0, 0], [3, 2, 1, 0], [2, 2, 1, 1],
+    [0, 0, 0, 0, 0], [1, 1, 0, 0, 0], [2, 2, 1, 1, 0], [4, 3, 2, 1, 0], [1, 1, 1, 1, 0],
+    [0] * 7, [1, 1, 1, 0, 0, 0, 2], [3, 3, 2, 2, 1, 1, 0], [6, 5, 4, 3, 2, 1, 0], [1, 1, 2, 2, 3, 3, 4],
+    [0, 0, 1, 1, 2, 2, 3, 3, 4], [8, 7, 6, 5, 4, 3, 2, 1, 0], [1] * 9, [0, 0, 0, 0, 1, 1, 1, 2, 3],
+    list(range(13)), [5, 5, 5, 3, 3, 1, 0, 0, 9, 9, 9, 9, 2],
+]
+
+
+def make_steps():
+    from photonic_engines.clifford import cuda_rect
+    from photonic_engines.clifford.variants import addends, cofactors_2020, step_amplitudes
+    rng = np.random.default_rng(2024)
+    blocks, rows_l, P64, Pld, T = [], [], [], [], []
+    for rows in PATTERNS:
+        K1 = len(rows)
+        K = K1 + 1
+        m = max(rows) + 1
+        A = rng.normal(size=(m, K)) + 1j * rng.normal(size=(m, K))       # one row of A per output mode
+        B = A[rows]                                                        # [K1, K]: equal modes -> equal rows
+        P, t = cofactors_2020(torch.tensor(B), rows)
+        Pl = cuda_rect.rect_cofactors_emul(torch.tensor(A[None]), torch.tensor([rows], dtype=torch.int64), K1,
+                                           real="long double", form="fock")
+        blocks.append(B); rows_l.append(rows); P64.append(P.numpy()); Pld.append(Pl[0].numpy()); T.append(t)
+        assert t == addends("2020", rows, list(range(K)))
+    # step amplitudes on the reference's test steps, U = haar(8, 1) (tests/clifford/test_variants.py:38-39)
+    U8 = haar(8, 1)
+    amps = [step_amplitudes(U8, r, c, "2020")[0].numpy() for r, c in STEPS]
+    pad = max(len(b) for b in rows_l) + 1
+    Bpad = np.zeros((len(blocks), pad - 1, pad), dtype=np.complex128)
+    Rpad = np.full((len(blocks), pad - 1), -1, dtype=np.int64)
+    P64p = np.zeros((len(blocks), pad), dtype=np.complex128)
+    Pldp = np.zeros((len(blocks), pad), dtype=np.complex128)
+    for i, (B, r, p, q) in enumerate(zip(blocks, rows_l, P64, Pld)):
+        Bpad[i, : B.shape[0], : B.shape[1]] = B
+        Rpad[i, : len(r)] = r
+        P64p[i, : p.shape[0]] = p
+        Pldp[i, : q.shape[0]] = q
+    np.savez_compressed(
+        os.path.join(HERE, "steps.npz"),
+        blocks=Bpad, rows=Rpad, K1=np.array([len(r) for r in rows_l]), P_f64=P64p, P_ld=Pldp, addends=np.array(T),
+        U8=U8.numpy(), step_rows=np.array([r + [-1] * (8 - len(r)) for r, _ in STEPS]),
+        step_cols=np.array([c + [-1] * (8 - len(c)) for _, c in STEPS]),
+        step_amps=np.array([np.pad(a, (0, 0)) for a in amps]))
+
+
+# (name, m, in_modes, B circuits, shots, generator seed, U seed, algo)
+CHAINS = [
+    ("n4m8", 8, [0, 1, 2, 3], 1, 64, 3, 3, "auto"),
+    ("bunched", 6, [0, 0, 2, 3], 1, 48, 11, 3, "2020"),
+    ("n6m12", 12, [0, 1, 2, 3, 4, 5], 1, 48, 5, 1001, "auto"),
+    ("batch2", 5, [0, 1, 2], 2, 24, 9, 21, "auto"),
+    ("n7m10_2020", 10, [0, 1, 2, 3, 4, 5, 6], 1, 24, 17, 33, "2020"),
+]
+# public fock_sample with imperfections: (name, m, in_modes, shots, generator seed, U seed, loss, indist)
+IMPERFECT = [
+    ("loss05", 8, [0, 1, 2, 3, 4], 64, 1, 5, 0.5, None),
+    ("indist095", 8, [0, 1, 2, 3, 4], 64, 2, 6, None, 0.95),
+    ("loss07_indist08", 9, [0, 1, 2, 3, 4, 5], 48, 3, 7, 0.7, 0.8),
+    ("indist_half_bunched", 7, [0, 0, 1, 2, 3], 48, 4, 8, None, 0.5),
+]
+
+
+def make_chains():
+    from photonic_engines.clifford import fock_sample
+    from photonic_engines.clifford import sampler as RS
+    from photonic_engines.clifford.cofactors_triton import cofactor_partials_multi
+    out = {}
+    for name, m, in_modes, Bn, shots, gseed, useed, algo in CHAINS:
+        U = torch.stack([haar(m, useed + b) for b in range(Bn)])
+        n = len(in_modes)
+        S = Bn * shots
+        A2 = torch.view_as_real(U[:, :, in_modes].to(torch.complex128).contiguous())
+        dp = torch.arange(Bn, dtype=torch.int64).repeat_interleave(shots)
+        gen = torch.Generator().manual_seed(gseed)
+        rows, _ = RS._sample_streams(A2, dp, n, m, gen, algo, 10, 1 << 16, 1 << 17, cofactor_partials_multi)
+        g2 = torch.Generator().manual_seed(gseed)
+        sig = torch.argsort(torch.rand(S, n, generator=g2), dim=1)
+        seeds = torch.randint(0, 2 ** 31 - 1, (n,), generator=g2)
+        occ = fock_sample(U if Bn > 1 else U[0], in_modes, shots, generator=torch.Generator().manual_seed(gseed),
+                          algo=algo)
+        out[f"{name}__U"] = U.numpy()
+        out[f"{name}__in_modes"] = np.array(in_modes)
+        out[f"{name}__meta"] = np.array([m, Bn, shots, gseed, useed])
+        out[f"{name}__sigma"] = sig.numpy()
+        out[f"{name}__seeds"] = seeds.numpy()
+        out[f"{name}__rows"] = rows.numpy()
+        out[f"{name}__occ"] = occ.numpy()
+        print(name, "rows", rows.shape, flush=True)
+    for name, m, in_modes, shots, gseed, useed, loss, indist in IMPERFECT:
+        U = haar(m, useed)
+        occ = fock_sample(U, in_modes, shots, generator=torch.Generator().manual_seed(gseed), loss=loss, indist=indist)
+        out[f"{name}__U"] = U.numpy()
+        out[f"{name}__in_modes"] = np.array(in_modes)
+        out[f"{name}__meta"] = np.array([m, shots, gseed, useed])
+        out[f"{name}__imperf"] = np.array([-1.0 if loss is None else loss, -1.0 if indist is None else indist])
+        out[f"{name}__occ"] = occ.numpy()
+        print(name, "occ", occ.shape, flush=True)
+    np.savez_compressed(os.path.join(HERE, "chains.npz"), **out)
+
+
+if __name__ == "__main__":
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PE_REFERENCE", "")
+    if not ref or not os.path.isdir(ref):
+        raise SystemExit("usage: make_golden.py /path/to/photonic-engines (the reference checkout)")
+    sys.path.insert(0, ref)
+    make_philox()
+    print("philox done", flush=True)
+    make_steps()
+    print("steps done", flush=True)
+    make_chains()
+    print("chains done", flush=True)

@@ -1,0 +1,75 @@
+"""Host-side logic of `fock_sample` on the CPU: the chain plan (sigma / seed draws, loss and partial
+distinguishability partition, grouping, singleton routing) must consume a seeded generator exactly as the
+reference does.  The oracle plays the chains of the plan, and the assembled occupations must equal the
+ones the reference's own `fock_sample` returned (tests/golden/chains.npz)."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN
+from oracle import oracle as O
+from photonic_engines_b200.clifford.sampler import assemble_occupations, plan_chains
+
+CHAINS = np.load(os.path.join(GOLDEN, "chains.npz"))
+LOSSLESS = sorted({k.split("__")[0] for k in CHAINS.files if k.endswith("__rows")})
+IMPERFECT = sorted({k.split("__")[0] for k in CHAINS.files if k.endswith("__imperf")})
+
+
+def _play(plan, U, in_modes):
+    """Run every chain of the plan on the oracle (grouped by photon count), then assemble occupations."""
+    A = U[:, :, in_modes].numpy()
+    rows = np.zeros((plan.C, plan.n), dtype=np.int64)
+    nk = np.full(plan.C, plan.n) if plan.nk is None else plan.nk.numpy()
+    for k in sorted(set(nk.tolist())):
+        sel = np.nonzero(nk == k)[0]
+        u = O.chain_uniforms(plan.seeds.numpy(), plan.seed_row.numpy()[sel], plan.rng_off.numpy()[sel], k)
+        out = O.chain(A, plan.dp.numpy()[sel], plan.cols.numpy()[sel, :k], u)
+        rows[sel, :k] = out["rows"]
+    return assemble_occupations(plan, torch.as_tensor(rows), U.shape[-1]).numpy()
+
+
+@pytest.mark.parametrize("name", LOSSLESS)
+def test_lossless_plan_reproduces_the_reference_samples(name):
+    U = torch.as_tensor(CHAINS[f"{name}__U"])
+    in_modes = CHAINS[f"{name}__in_modes"].tolist()
+    m, Bn, shots, gseed = CHAINS[f"{name}__meta"][:4].tolist()
+    S = Bn * shots
+    dp_all = torch.arange(Bn).repeat_interleave(shots)
+    plan = plan_chains(U, in_modes, S, dp_all, torch.Generator().manual_seed(gseed), None, None, 1 << 18)
+    assert torch.equal(plan.cols, torch.as_tensor(CHAINS[f"{name}__sigma"]))
+    assert torch.equal(plan.seeds[0], torch.as_tensor(CHAINS[f"{name}__seeds"]))
+    assert np.array_equal(_play(plan, U, in_modes), CHAINS[f"{name}__occ"])
+
+
+def test_max_streams_splits_a_pass_into_chunks_with_their_own_draws():
+    U = torch.as_tensor(O.haar_unitary(6, 2))[None]
+    plan = plan_chains(U, [0, 1, 2], 10, torch.zeros(10, dtype=torch.int64), torch.Generator().manual_seed(1),
+                       None, None, 4)
+    assert plan.seeds.shape == (3, 3)
+    assert plan.seed_row.tolist() == [0] * 4 + [1] * 4 + [2] * 2
+    assert plan.rng_off.tolist() == [0, 1, 2, 3, 0, 1, 2, 3, 0, 1]
+
+
+@pytest.mark.parametrize("name", IMPERFECT)
+def test_imperfect_plan_reproduces_the_reference_samples(name):
+    U = torch.as_tensor(CHAINS[f"{name}__U"])
+    in_modes = CHAINS[f"{name}__in_modes"].tolist()
+    m, shots, gseed = CHAINS[f"{name}__meta"][:3].tolist()
+    loss, indist = CHAINS[f"{name}__imperf"].tolist()
+    loss = None if loss < 0 else loss
+    indist = None if indist < 0 else indist
+    plan = plan_chains(U[None], in_modes, shots, torch.zeros(shots, dtype=torch.int64),
+                       torch.Generator().manual_seed(gseed), loss, indist, 1 << 18)
+    occ = _play(plan, U[None], in_modes)
+    assert np.array_equal(occ, CHAINS[f"{name}__occ"])
+    assert (occ.sum(1) <= len(in_modes)).all()
+
+
+def test_loss_zero_transmission_returns_empty_samples():
+    U = torch.as_tensor(O.haar_unitary(5, 3))[None]
+    plan = plan_chains(U, [0, 1, 2], 8, torch.zeros(8, dtype=torch.int64), torch.Generator().manual_seed(0), 0.0,
+                       None, 1 << 18)
+    assert plan.C == 0 and plan.single_ids is None
+    assert assemble_occupations(plan, None, 5).sum() == 0
