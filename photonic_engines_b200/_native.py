@@ -11,7 +11,7 @@ import os
 import torch
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libpe_b200.so")
+LIB_PATH = os.environ.get("PE_LIB", os.path.join(_HERE, "libpe_b200.so"))
 
 PE_OK = 0
 PE_PRECISION_F64 = 0

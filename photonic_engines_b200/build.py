@@ -3,6 +3,8 @@
 Every kernel variant (precision x threads per Gray lane x largest column tier) is one object file
 compiled from csrc/fock_inst.cu with its own -D flags, in parallel; csrc/fock_api.cu holds the C ABI.
 Objects are rebuilt only when a source is newer.  `python -m photonic_engines_b200.build` builds it.
+Environment: PE_NVCC_FLAGS (extra nvcc flags, e.g. tuning macros), PE_BUILD_DIR (object directory),
+PE_LIB (output library path; the loader reads the same variable).
 """
 from __future__ import annotations
 
@@ -14,15 +16,18 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-OBJ = os.path.join(HERE, "_build")
-LIB = os.path.join(HERE, "libpe_b200.so")
+OBJ = os.environ.get("PE_BUILD_DIR", os.path.join(HERE, "_build"))
+LIB = os.environ.get("PE_LIB", os.path.join(HERE, "libpe_b200.so"))
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc" if os.path.exists("/usr/local/cuda/bin/nvcc") else "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include"), "-I", CSRC]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+         *os.environ.get("PE_NVCC_FLAGS", "").split()]
 
 # (mixed, threads per lane, largest tier) of every compiled chain/cofactor kernel pair
 VARIANTS = [(mx, tpl, kpm) for mx in (0, 1) for tpl, kpms in ((1, (8, 16)), (2, (8, 16, 20, 24, 28, 32)),
                                                               (4, (8, 16, 20, 24, 28, 32))) for kpm in kpms]
+if os.environ.get("PE_VARIANTS"):          # a subset "m,t,k;m,t,k" (experiments: smaller, faster builds)
+    VARIANTS = [tuple(int(x) for x in v.split(",")) for v in os.environ["PE_VARIANTS"].split(";")]
 
 
 def _sources():

@@ -163,7 +163,7 @@ extern "C" int pe_fock_chain(int precision, const double* d_acol, const int64_t*
     p.status = (int*)((char*)d_workspace + 8);
     p.detail = (long long*)((char*)d_workspace + 16);
     p.m_cap = m_max;
-    p.tau = 2.0e-6;
+    p.tau = 3.0e-5;
     void* args[] = {&p};
     if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st) != cudaSuccess) return PE_ERR_CUDA;
     return PE_OK;

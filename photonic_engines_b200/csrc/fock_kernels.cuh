@@ -2,10 +2,11 @@
 // chains, one CTA per stream at a time (a work queue hands out streams), everything of a step in
 // shared memory and registers:
 //
-//   plan     thread 0: multiplicity tables of the chosen rows, halving rule, term count, and the
-//            split of the collapsed Gray sum into CTA-uniform inner blocks, middle blocks and lanes
+//   plan     warp 0: radices of the collapsed sum from the chosen rows' multiplicities (kept
+//            incrementally), halving rule, term count, and the split of the sum into CTA-uniform
+//            inner blocks, middle blocks and Gray lanes
 //   prepare  all threads: gather B = A[chosen rows, sigma(1..k)] into shared memory, fill the inner
-//            Gray schedule (digit, sign, exact weight per term)
+//            and middle Gray schedules (digit, sign, exact weight per index)
 //   sweep    every Gray lane walks its terms; the row flipped at a term is the same for the whole
 //            CTA (broadcast shared-memory reads, no divergence); all-but-one products by prefix and
 //            suffix chains, split over TPL threads per lane; deterministic warp/CTA reduction
@@ -13,7 +14,7 @@
 //            CDF pick with the reference's rule, Philox uniforms identical to the reference's
 //
 // FP64 form: complex FP64 throughout.  Mixed form: inner blocks in complex FP32 (column sums
-// re-initialised from FP64 at every block start), block sums folded into FP64 accumulators, FP64
+// formed in FP64 at every block start), block sums folded into FP64 accumulators, FP64
 // cross-lane reduction, marginal and CDF; a draw that falls within a guard band of a CDF step is
 // recomputed with the FP64 sweep, so the mixed form picks what the FP64 form picks.
 //
@@ -28,6 +29,16 @@
 
 #include "pe_b200.h"
 #include "pe_device.cuh"
+
+#ifndef PE_UNROLL
+#define PE_UNROLL 1         // Gray terms per inner-loop iteration (1 or 2)
+#endif
+#ifndef PE_SPLIT
+#define PE_SPLIT 1          // FP64: split a thread's product chain in two interleaved halves (1-/2-thread lanes)
+#endif
+#ifndef PE_MINB
+#define PE_MINB 2           // resident 256-thread CTAs per SM the register allocation must allow
+#endif
 
 namespace pe {
 
@@ -59,6 +70,12 @@ struct ChainParams {
     double tau;     // mixed form: relative guard band of the draw
 };
 
+// Mixed form: FP32 inner blocks of at most this many terms, each starting from FP64 column sums.
+#ifndef PE_MIXED_LIN
+#define PE_MIXED_LIN 512
+#endif
+constexpr int MIXED_LIN = PE_MIXED_LIN;
+
 // Workspace layout: [0] queue counter (u64), [8] status (i32), [16] detail (i64).  Zeroed per call.
 constexpr size_t WS_BYTES = 256;
 
@@ -66,84 +83,139 @@ static __device__ __forceinline__ void record_error(int* status, long long* deta
     if (atomicCAS(status, 0, PE_ERR_DEVICE) == 0) *detail = (long long)s;
 }
 
+// ---------------------------------------------------------------------------------------- groups
+// Thread 0, after every pick: the distinct chosen modes and their multiplicities (the grouping of
+// cofactors_triton.py:419-427, kept incrementally instead of re-sorting the rows every step).
+static __device__ __forceinline__ void add_to_groups(Smem& sm, int row) {
+    for (int g = 0; g < sm.ngrp; ++g)
+        if (sm.grow[g] == row) { sm.gmul[g] += 1; return; }
+    sm.grow[sm.ngrp] = row;
+    sm.gmul[sm.ngrp] = 1;
+    sm.ngrp += 1;
+}
+
 // ---------------------------------------------------------------------------------------- plan
-// Thread 0.  Multiplicity tables exactly as the reference builds them (sort, group, move the last
-// odd group to the top slot, radix = mult + 1, top radix halved when an odd group exists), then
-// the kernel's own enumeration split.  The order in which digits are enumerated does not change
-// the sum; only the set of radices (hence N) is the reference's.
-static __device__ void plan_step(Plan& pl, const int* rows, int K1, int K, int lanes) {
-    int rs[MAXN];
-    for (int i = 0; i < K1; ++i) rs[i] = rows[i];
-    for (int i = 1; i < K1; ++i) {
-        const int x = rs[i];
-        int j = i - 1;
-        while (j >= 0 && rs[j] > x) { rs[j + 1] = rs[j]; --j; }
-        rs[j + 1] = x;
+// Warp 0.  Lane g holds group g.  Radix = mult + 1, and one odd-multiplicity group (the last one)
+// has its radix halved to (mult + 1) / 2 with the scale doubled — the complement symmetry
+// v -> s - v of the reference (cofactors_triton.py:428-446); which odd group is halved does not
+// change N or the sum.  Active digits (radix >= 2) are ranked by ascending radix; the leading ones
+// become the Gray lanes (best fill of the CTA's lanes), the next ones the inner block, then the
+// middle block; what does not fit the schedules joins the lanes.
+static __device__ void plan_step(Smem& sm, int K1, int K, int lanes, int lin_max) {
+    Plan& pl = sm.plan;
+    const int lane = threadIdx.x & 31;
+    const int D = sm.ngrp;
+    const bool has = lane < D;
+    const int M = has ? sm.gmul[lane] : 0;
+    const unsigned oddmask = __ballot_sync(0xffffffffu, has && (M & 1));
+    const int halved = oddmask ? 31 - __clz(oddmask) : -1;
+    const int R = has ? (lane == halved ? (M + 1) / 2 : M + 1) : 1;
+    const bool active = R >= 2;
+    int rank = 0;
+    for (int j = 0; j < 32; ++j) {
+        const int Rj = __shfl_sync(0xffffffffu, R, j);
+        if (Rj >= 2 && active && (Rj < R || (Rj == R && j < lane))) ++rank;
     }
-    int drow[MAXN], mult[MAXN], radix[MAXN];
-    int D = 0;
-    for (int i = 0; i < K1; ++i) {
-        if (D > 0 && drow[D - 1] == rs[i]) mult[D - 1]++;
-        else { drow[D] = rs[i]; mult[D] = 1; ++D; }
-    }
-    int pos = -1;
-    for (int q = 0; q < D; ++q) if (mult[q] & 1) pos = q;
-    if (pos >= 0 && pos != D - 1) {
-        int t = drow[pos]; drow[pos] = drow[D - 1]; drow[D - 1] = t;
-        t = mult[pos]; mult[pos] = mult[D - 1]; mult[D - 1] = t;
-    }
-    int64_t N = 1;
-    for (int q = 0; q < D; ++q) {
-        radix[q] = (q == D - 1 && pos >= 0) ? (mult[q] + 1) / 2 : mult[q] + 1;
-        N *= radix[q];
-    }
-    // active digits (radix >= 2) by ascending radix; radix-1 digits are fixed
-    int act[MAXN], na = 0, fix[MAXN], nf = 0;
-    for (int q = 0; q < D; ++q) {
-        if (radix[q] >= 2) {
-            int j = na++;
-            while (j > 0 && radix[act[j - 1]] > radix[q]) { act[j] = act[j - 1]; --j; }
-            act[j] = q;
-        } else {
-            fix[nf++] = q;
+    if (active) { pl.sortR[rank] = R; pl.sortG[rank] = lane; }
+    __syncwarp();
+    const unsigned actmask = __ballot_sync(0xffffffffu, active);
+    if (lane == 0) {
+        const int na = __popc(actmask);
+        int64_t N = 1;
+        for (int i = 0; i < na; ++i) N *= pl.sortR[i];
+        // lanes: the prefix of the ranked digits that best fills the CTA's lanes
+        int nhi = na;
+        if (N > lanes) {
+            double best = -1.0;
+            int64_t prod = 1;
+            nhi = 1;
+            for (int i = 0; i < na; ++i) {
+                prod *= pl.sortR[i];
+                if (i > 0 && N / prod < 4) break;
+                const double e = prod >= lanes
+                    ? (double)prod / ((double)lanes * (double)((prod + lanes - 1) / lanes))
+                    : (double)prod / (double)lanes;
+                if (e > best + 1e-12) { best = e; nhi = i + 1; }
+                if (prod >= lanes && e >= 0.95) break;
+            }
         }
-    }
-    // high digits: the prefix of `act` whose product best fills the lanes
-    int nhi = na;
-    int64_t H = N;
-    if (N > lanes) {
-        double best = -1.0;
-        int64_t prod = 1;
-        nhi = 1;
-        for (int i = 0; i < na; ++i) {
-            prod *= radix[act[i]];
-            if (i > 0 && N / prod < 4) break;
-            const double e = prod >= lanes
-                ? (double)prod / ((double)lanes * (double)((prod + lanes - 1) / lanes))
-                : (double)prod / (double)lanes;
-            if (e > best + 1e-12) { best = e; nhi = i + 1; }
-            if (prod >= lanes && e >= 0.95) break;
+        int nin = 0, Lin = 1;
+        while (nhi + nin < na && Lin * pl.sortR[nhi + nin] <= lin_max) { Lin *= pl.sortR[nhi + nin]; ++nin; }
+        int nmid = 0, Lmid = 1;
+        while (nhi + nin + nmid < na && Lmid * pl.sortR[nhi + nin + nmid] <= MID_MAX) {
+            Lmid *= pl.sortR[nhi + nin + nmid];
+            ++nmid;
         }
-        H = 1;
-        for (int i = 0; i < nhi; ++i) H *= radix[act[i]];
+        const int nextra = na - nhi - nin - nmid;       // digits beyond both schedules: more lanes
+        int kd = 0;
+        for (int i = 0; i < nin; ++i, ++kd) {
+            const int g = pl.sortG[nhi + i];
+            pl.R[kd] = pl.sortR[nhi + i];
+            pl.Pin[kd] = (kd == 0) ? 1 : pl.Pin[kd - 1] * pl.R[kd - 1];
+            pl.M[kd] = sm.gmul[g];
+            pl.drow[kd] = sm.grow[g];
+        }
+        for (int i = 0; i < nmid; ++i, ++kd) {
+            const int g = pl.sortG[nhi + nin + i];
+            pl.R[kd] = pl.sortR[nhi + nin + i];
+            pl.Pmid[i] = (i == 0) ? 1 : pl.Pmid[i - 1] * pl.R[kd - 1];
+            pl.M[kd] = sm.gmul[g];
+            pl.drow[kd] = sm.grow[g];
+        }
+        int64_t H = 1;
+        for (int i = 0; i < nhi; ++i, ++kd) {
+            const int g = pl.sortG[i];
+            pl.R[kd] = pl.sortR[i];
+            pl.M[kd] = sm.gmul[g];
+            pl.drow[kd] = sm.grow[g];
+            H *= pl.R[kd];
+        }
+        for (int i = 0; i < nextra; ++i, ++kd) {
+            const int g = pl.sortG[nhi + nin + nmid + i];
+            pl.R[kd] = pl.sortR[nhi + nin + nmid + i];
+            pl.M[kd] = sm.gmul[g];
+            pl.drow[kd] = sm.grow[g];
+            H *= pl.R[kd];
+        }
+        for (int g = 0; g < D; ++g) {                    // fixed digits: radix 1
+            int Rg = (g == halved) ? (sm.gmul[g] + 1) / 2 : sm.gmul[g] + 1;
+            if (Rg < 2) { pl.R[kd] = 1; pl.M[kd] = sm.gmul[g]; pl.drow[kd] = sm.grow[g]; ++kd; }
+        }
+        pl.N = N; pl.H = H; pl.Lin = Lin; pl.Lmid = Lmid;
+        pl.K = K; pl.K1 = K1; pl.D = D;
+        pl.nin = nin; pl.nmid = nmid; pl.nhi = nhi + nextra;
+        pl.scale = (halved >= 0 ? 2.0 : 1.0) * ldexp(1.0, -K1);
     }
-    // inner: leading low digits while the block fits the schedule table; the rest are middle
-    int nin = 0, Lin = 1;
-    while (nhi + nin < na && Lin * radix[act[nhi + nin]] <= LIN_MAX) { Lin *= radix[act[nhi + nin]]; ++nin; }
-    const int nmid = na - nhi - nin;
-    int64_t Lmid = 1;
-    int kd = 0;
-    for (int i = 0; i < nin; ++i, ++kd) { const int q = act[nhi + i]; pl.R[kd] = radix[q]; pl.M[kd] = mult[q]; pl.drow[kd] = drow[q]; }
-    for (int i = 0; i < nmid; ++i, ++kd) { const int q = act[nhi + nin + i]; pl.R[kd] = radix[q]; pl.M[kd] = mult[q]; pl.drow[kd] = drow[q]; Lmid *= radix[q]; }
-    for (int i = 0; i < nhi; ++i, ++kd) { const int q = act[i]; pl.R[kd] = radix[q]; pl.M[kd] = mult[q]; pl.drow[kd] = drow[q]; }
-    for (int i = 0; i < nf; ++i, ++kd) { const int q = fix[i]; pl.R[kd] = 1; pl.M[kd] = mult[q]; pl.drow[kd] = drow[q]; }
-    pl.N = N; pl.H = H; pl.Lmid = Lmid; pl.Lin = Lin;
-    pl.K = K; pl.K1 = K1; pl.D = D;
-    pl.nin = nin; pl.nmid = nmid; pl.nhi = nhi;
-    pl.scale = (pos >= 0 ? 2.0 : 1.0) * ldexp(1.0, -K1);
 }
 
 // ---------------------------------------------------------------------------------------- prepare
+// One index of a reflected mixed-radix Gray schedule over `nd` digits starting at kernel digit
+// `d0` with radices R and prefix products Pp: its weight prod (-1)^v C(M, v) and the transition
+// into it (the digit the odometer moved, and the sign of the column-sum update -2 dir b).
+static __device__ __forceinline__ unsigned char gray_entry(const Plan& pl, int d0, int nd, const int* Pp, int t,
+                                                          double* w_out, unsigned char* vend) {
+    int qstar = -1;
+    if (t > 0) {
+        for (int q = 0; q < nd; ++q)
+            if ((t / Pp[q]) % pl.R[d0 + q] != 0) { qstar = q; break; }
+    }
+    int par = 0, parh = 0;
+    double w = 1.0;
+    for (int q = nd - 1; q >= 0; --q) {
+        if (q == qstar) parh = par;
+        const int R = pl.R[d0 + q];
+        const int d = (t / Pp[q]) % R;
+        const int v = (par & 1) ? R - 1 - d : d;
+        if (vend) vend[q] = (unsigned char)v;
+        par += v;
+        w *= signed_binom(pl.M[d0 + q], v);
+    }
+    *w_out = w;
+    if (qstar < 0) return 0;
+    const int dir = (parh & 1) ? -1 : 1;            // v moved by dir: column sums move by -2 dir b
+    return (unsigned char)(qstar | (dir > 0 ? 0x80 : 0));
+}
+
 // All threads.  Element (rho, j) of the instance is A[rho * rs + j * cs].
 static __device__ void prepare_step(Smem& sm, const double2* __restrict__ A, int64_t rs, int64_t cs, bool mixed) {
     const Plan& pl = sm.plan;
@@ -155,46 +227,76 @@ static __device__ void prepare_step(Smem& sm, const double2* __restrict__ A, int
         sm.B[kd][j] = b;
         if (mixed) sm.B32[kd][j] = make_float2((float)(2.0 * b.x), (float)(2.0 * b.y));
     }
-    const int nin = pl.nin;
     for (int t = tid; t < pl.Lin; t += T) {
-        int d[MAXN], v[MAXN];
-        int rem = t;
-        for (int q = 0; q < nin; ++q) { d[q] = rem % pl.R[q]; rem /= pl.R[q]; }
-        int par = 0;
-        for (int q = nin - 1; q >= 0; --q) { v[q] = (par & 1) ? pl.R[q] - 1 - d[q] : d[q]; par += v[q]; }
-        double w = 1.0;
-        for (int q = 0; q < nin; ++q) w *= signed_binom(pl.M[q], v[q]);
+        double w;
+        sm.tab_f[t] = gray_entry(pl, 0, pl.nin, pl.Pin, t, &w, t == pl.Lin - 1 ? sm.plan.vend : nullptr);
         sm.tab_w[t] = w;
         sm.tab_w32[t] = (float)w;
-        unsigned char e = 0;
-        if (t > 0) {
-            int q = 0;
-            while (d[q] == 0) ++q;                       // the digit the odometer moved
-            int parh = 0;
-            for (int mu = q + 1; mu < nin; ++mu) parh += v[mu];
-            const int dir = (parh & 1) ? -1 : 1;         // v_q moved by dir: column sums move by -2 dir b_q
-            e = (unsigned char)(q | (dir > 0 ? 0x80 : 0));
-        }
-        sm.tab_f[t] = e;
-        if (t == pl.Lin - 1)
-            for (int q = 0; q < nin; ++q) sm.plan.vend[q] = (unsigned char)v[q];
+    }
+    for (int t = tid; t < pl.Lmid; t += T) {
+        double w;
+        sm.tab_fm[t] = gray_entry(pl, pl.nin, pl.nmid, pl.Pmid, t, &w, nullptr);
+        sm.tab_wm[t] = w;
     }
 }
 
+// Middle digit values at middle index pm (the reflected Gray code decoded directly).
+static __device__ __forceinline__ int middle_digit(const Plan& pl, int pm, int q) {
+    int par = 0, v = 0;
+    for (int i = pl.nmid - 1; i >= q; --i) {
+        const int R = pl.R[pl.nin + i];
+        const int d = (pm / pl.Pmid[i]) % R;
+        v = (par & 1) ? R - 1 - d : d;
+        par += v;
+    }
+    return v;
+}
+
 // ---------------------------------------------------------------------------------------- sweep
-// acc_c += w * prod_{j != c} s_j over this thread's KH columns; the other TPL - 1 threads of the
-// lane contribute the product of their columns (exchanged once per term).  w enters the prefix
-// chain of the lane's first thread.
-template <int KH, int TPL, typename R>
-__device__ __forceinline__ void allbutone_acc(const R (&sr)[KH], const R (&si)[KH], R w, R (&ar)[KH], R (&ai)[KH],
-                                              int h, unsigned gmask) {
+template <int TPL>
+__device__ __forceinline__ unsigned group_mask() {
+    if constexpr (TPL == 1) return 0u;
+    else return ((1u << TPL) - 1u) << ((threadIdx.x & 31) & ~(TPL - 1));
+}
+
+// Product of the other three threads' totals of a 4-thread lane: all three are gathered with
+// independent shuffles (one shuffle latency), then multiplied.
+template <int TPL, typename R>
+__device__ __forceinline__ void others_product(R xr, R xi, R& yr, R& yi, unsigned gmask) {
+    const R ar = __shfl_xor_sync(gmask, xr, 1), ai = __shfl_xor_sync(gmask, xi, 1);
+    const R br = __shfl_xor_sync(gmask, xr, 2), bi = __shfl_xor_sync(gmask, xi, 2);
+    const R cr = __shfl_xor_sync(gmask, xr, 3), ci = __shfl_xor_sync(gmask, xi, 3);
+    const R tr = fma(ar, br, -(ai * bi)), ti = fma(ar, bi, ai * br);
+    yr = fma(tr, cr, -(ti * ci));
+    yi = fma(tr, ci, ti * cr);
+}
+
+// One term: optional rank-1 update of the column sums (brow != null: s += f b), then
+// acc_c += w prod_{j != c} s_j over this thread's KH columns.  The product of the other TPL - 1
+// threads' columns of the lane enters the suffix chain (exchanged once per term); w enters the
+// prefix chain of the lane's first thread.
+template <int KH, int TPL, typename R, typename C2>
+__device__ __forceinline__ void term(R (&sr)[KH], R (&si)[KH], R (&ar)[KH], R (&ai)[KH], const C2* brow, R f, R w,
+                                     int h, unsigned gmask) {
     R pr[KH], pi[KH];
-    R xr = (h == 0) ? w : R(1), xi = R(0);
+    if (brow) {
 #pragma unroll
-    for (int c = 0; c < KH; ++c) {
-        pr[c] = xr; pi[c] = xi;
-        const R nr = xr * sr[c] - xi * si[c];
-        xi = xr * si[c] + xi * sr[c];
+        for (int c = 0; c < KH; ++c) {
+            const C2 b = brow[c];
+            sr[c] = fma(f, (R)b.x, sr[c]);
+            si[c] = fma(f, (R)b.y, si[c]);
+        }
+    }
+    const R w0 = (h == 0) ? w : R(1);
+    pr[0] = w0;
+    pi[0] = R(0);
+    R xr = w0 * sr[0], xi = w0 * si[0];
+#pragma unroll
+    for (int c = 1; c < KH; ++c) {
+        pr[c] = xr;
+        pi[c] = xi;
+        const R nr = fma(xr, sr[c], -(xi * si[c]));
+        xi = fma(xr, si[c], xi * sr[c]);
         xr = nr;
     }
     R yr, yi;
@@ -204,19 +306,211 @@ __device__ __forceinline__ void allbutone_acc(const R (&sr)[KH], const R (&si)[K
         yr = __shfl_xor_sync(gmask, xr, 1);
         yi = __shfl_xor_sync(gmask, xi, 1);
     } else {
-        const R qr = __shfl_xor_sync(gmask, xr, 1), qi = __shfl_xor_sync(gmask, xi, 1);
-        const R pr2 = xr * qr - xi * qi, pi2 = xr * qi + xi * qr;
-        const R orr = __shfl_xor_sync(gmask, pr2, 2), oi = __shfl_xor_sync(gmask, pi2, 2);
-        yr = qr * orr - qi * oi;
-        yi = qr * oi + qi * orr;
+        others_product<TPL>(xr, xi, yr, yi, gmask);
     }
 #pragma unroll
-    for (int c = KH - 1; c >= 0; --c) {
-        ar[c] += pr[c] * yr - pi[c] * yi;
-        ai[c] += pr[c] * yi + pi[c] * yr;
-        const R nr = yr * sr[c] - yi * si[c];
-        yi = yr * si[c] + yi * sr[c];
+    for (int c = KH - 1; c >= 1; --c) {
+        ar[c] = fma(pr[c], yr, ar[c]);
+        ar[c] = fma(-pi[c], yi, ar[c]);
+        ai[c] = fma(pr[c], yi, ai[c]);
+        ai[c] = fma(pi[c], yr, ai[c]);
+        const R nr = fma(yr, sr[c], -(yi * si[c]));
+        yi = fma(yr, si[c], yi * sr[c]);
         yr = nr;
+    }
+    ar[0] = fma(pr[0], yr, ar[0]);
+    ai[0] = fma(pr[0], yi, ai[0]);
+}
+
+// One term with this thread's KH columns split into two halves A = [0, KA) and B = [KA, KH) whose
+// product chains run interleaved (two independent dependency chains instead of one).  The half
+// totals are folded into the other half's suffix start, so for TPL == 1 this costs no extra
+// multiplication; for TPL == 2 the lane total, and the two suffix starts, cost three.
+template <int KH, int TPL, typename R, typename C2>
+__device__ __forceinline__ void term_split(R (&sr)[KH], R (&si)[KH], R (&ar)[KH], R (&ai)[KH], const C2* brow, R f,
+                                           R w, int h, unsigned gmask) {
+    constexpr int KA = KH / 2;
+    R pr[KH], pi[KH];
+    if (brow) {
+#pragma unroll
+        for (int c = 0; c < KH; ++c) {
+            const C2 b = brow[c];
+            sr[c] = fma(f, (R)b.x, sr[c]);
+            si[c] = fma(f, (R)b.y, si[c]);
+        }
+    }
+    const R w0 = (h == 0) ? w : R(1);
+    pr[0] = w0; pi[0] = R(0);
+    pr[KA] = R(1); pi[KA] = R(0);
+    R xar = w0 * sr[0], xai = w0 * si[0];
+    R xbr = sr[KA], xbi = si[KA];
+#pragma unroll
+    for (int i = 1; i < KH - KA; ++i) {
+        if (i < KA) {
+            const int c = i;
+            pr[c] = xar; pi[c] = xai;
+            const R nr = fma(xar, sr[c], -(xai * si[c]));
+            xai = fma(xar, si[c], xai * sr[c]);
+            xar = nr;
+        }
+        {
+            const int c = KA + i;
+            pr[c] = xbr; pi[c] = xbi;
+            const R nr = fma(xbr, sr[c], -(xbi * si[c]));
+            xbi = fma(xbr, si[c], xbi * sr[c]);
+            xbr = nr;
+        }
+    }
+    R yar, yai, ybr, ybi;                 // suffix starts: other half's total times the other threads'
+    if constexpr (TPL == 1) {
+        yar = xbr; yai = xbi;
+        ybr = xar; ybi = xai;
+    } else {
+        const R tr = fma(xar, xbr, -(xai * xbi)), ti = fma(xar, xbi, xai * xbr);
+        const R Yr = __shfl_xor_sync(gmask, tr, 1), Yi = __shfl_xor_sync(gmask, ti, 1);
+        yar = fma(xbr, Yr, -(xbi * Yi)); yai = fma(xbr, Yi, xbi * Yr);
+        ybr = fma(xar, Yr, -(xai * Yi)); ybi = fma(xar, Yi, xai * Yr);
+    }
+#pragma unroll
+    for (int i = KH - KA - 1; i >= 1; --i) {
+        {
+            const int c = KA + i;
+            ar[c] = fma(pr[c], ybr, ar[c]);
+            ar[c] = fma(-pi[c], ybi, ar[c]);
+            ai[c] = fma(pr[c], ybi, ai[c]);
+            ai[c] = fma(pi[c], ybr, ai[c]);
+            const R nr = fma(ybr, sr[c], -(ybi * si[c]));
+            ybi = fma(ybr, si[c], ybi * sr[c]);
+            ybr = nr;
+        }
+        if (i < KA) {
+            const int c = i;
+            ar[c] = fma(pr[c], yar, ar[c]);
+            ar[c] = fma(-pi[c], yai, ar[c]);
+            ai[c] = fma(pr[c], yai, ai[c]);
+            ai[c] = fma(pi[c], yar, ai[c]);
+            const R nr = fma(yar, sr[c], -(yai * si[c]));
+            yai = fma(yar, si[c], yai * sr[c]);
+            yar = nr;
+        }
+    }
+    ar[KA] = fma(pr[KA], ybr, ar[KA]);
+    ai[KA] = fma(pr[KA], ybi, ai[KA]);
+    ar[0] = fma(pr[0], yar, ar[0]);
+    ai[0] = fma(pr[0], yai, ai[0]);
+}
+
+// Term dispatch: split chains for wide per-thread column sets of 1- or 2-thread lanes.
+template <int KH, int TPL, typename R, typename C2>
+__device__ __forceinline__ void term_any(R (&sr)[KH], R (&si)[KH], R (&ar)[KH], R (&ai)[KH], const C2* brow, R f, R w,
+                                         int h, unsigned gmask) {
+    if constexpr (PE_SPLIT && sizeof(R) == 8 && TPL <= 2 && KH >= 6)
+        term_split<KH, TPL, R, C2>(sr, si, ar, ai, brow, f, w, h, gmask);
+    else term<KH, TPL, R, C2>(sr, si, ar, ai, brow, f, w, h, gmask);
+}
+
+// Two consecutive terms, interleaved for instruction-level parallelism: the first applies the
+// update (fa, ba) to s, the second (fb, bb) on top of it; their product chains are independent.
+template <int KH, int TPL, typename R, typename C2>
+__device__ __forceinline__ void term2(R (&sr)[KH], R (&si)[KH], R (&ar)[KH], R (&ai)[KH], const C2* ba, R fa, R wa,
+                                      const C2* bb, R fb, R wb, int h, unsigned gmask) {
+    R tr[KH], ti[KH];
+#pragma unroll
+    for (int c = 0; c < KH; ++c) {
+        const C2 x = ba[c], y = bb[c];
+        sr[c] = fma(fa, (R)x.x, sr[c]);
+        si[c] = fma(fa, (R)x.y, si[c]);
+        tr[c] = fma(fb, (R)y.x, sr[c]);
+        ti[c] = fma(fb, (R)y.y, si[c]);
+    }
+    R par[KH], pai[KH], pbr[KH], pbi[KH];
+    const R wa0 = (h == 0) ? wa : R(1), wb0 = (h == 0) ? wb : R(1);
+    par[0] = wa0; pai[0] = R(0);
+    pbr[0] = wb0; pbi[0] = R(0);
+    R xar = wa0 * sr[0], xai = wa0 * si[0];
+    R xbr = wb0 * tr[0], xbi = wb0 * ti[0];
+#pragma unroll
+    for (int c = 1; c < KH; ++c) {
+        par[c] = xar; pai[c] = xai;
+        pbr[c] = xbr; pbi[c] = xbi;
+        const R nar = fma(xar, sr[c], -(xai * si[c]));
+        xai = fma(xar, si[c], xai * sr[c]);
+        xar = nar;
+        const R nbr = fma(xbr, tr[c], -(xbi * ti[c]));
+        xbi = fma(xbr, ti[c], xbi * tr[c]);
+        xbr = nbr;
+    }
+    R yar, yai, ybr, ybi;
+    if constexpr (TPL == 1) {
+        yar = R(1); yai = R(0); ybr = R(1); ybi = R(0);
+    } else if constexpr (TPL == 2) {
+        yar = __shfl_xor_sync(gmask, xar, 1);
+        yai = __shfl_xor_sync(gmask, xai, 1);
+        ybr = __shfl_xor_sync(gmask, xbr, 1);
+        ybi = __shfl_xor_sync(gmask, xbi, 1);
+    } else {
+        others_product<TPL>(xar, xai, yar, yai, gmask);
+        others_product<TPL>(xbr, xbi, ybr, ybi, gmask);
+    }
+#pragma unroll
+    for (int c = KH - 1; c >= 1; --c) {
+        ar[c] = fma(par[c], yar, ar[c]);
+        ar[c] = fma(-pai[c], yai, ar[c]);
+        ai[c] = fma(par[c], yai, ai[c]);
+        ai[c] = fma(pai[c], yar, ai[c]);
+        ar[c] = fma(pbr[c], ybr, ar[c]);
+        ar[c] = fma(-pbi[c], ybi, ar[c]);
+        ai[c] = fma(pbr[c], ybi, ai[c]);
+        ai[c] = fma(pbi[c], ybr, ai[c]);
+        const R nar = fma(yar, sr[c], -(yai * si[c]));
+        yai = fma(yar, si[c], yai * sr[c]);
+        yar = nar;
+        const R nbr = fma(ybr, tr[c], -(ybi * ti[c]));
+        ybi = fma(ybr, ti[c], ybi * tr[c]);
+        ybr = nbr;
+    }
+    ar[0] = fma(par[0], yar, ar[0]);
+    ai[0] = fma(par[0], yai, ai[0]);
+    ar[0] = fma(pbr[0], ybr, ar[0]);
+    ai[0] = fma(pbr[0], ybi, ai[0]);
+#pragma unroll
+    for (int c = 0; c < KH; ++c) { sr[c] = tr[c]; si[c] = ti[c]; }
+}
+
+// Walk one inner block forward (fwd) or backward from the current column sums.  `f2` is the
+// magnitude of the column-sum step (2 for B, 1 for the pre-doubled B32); w_t = wscale * tab[t].
+template <int KH, int TPL, int UNR, typename R, typename C2, typename TabW>
+__device__ __forceinline__ void inner_block(R (&sr)[KH], R (&si)[KH], R (&ar)[KH], R (&ai)[KH], const Smem& sm,
+                                           const C2 (*Bm)[MAXN], const TabW* tab, R wscale, R f2, bool fwd, int Lin,
+                                           int c0, int h, unsigned gmask) {
+    if (fwd) {
+        term_any<KH, TPL, R, C2>(sr, si, ar, ai, nullptr, R(0), wscale * (R)tab[0], h, gmask);
+        int t = 1;
+        if constexpr (UNR == 2) {
+            for (; t + 1 < Lin; t += 2) {
+                const unsigned ea = sm.tab_f[t], eb = sm.tab_f[t + 1];
+                term2<KH, TPL, R, C2>(sr, si, ar, ai, &Bm[ea & 63u][c0], (ea & 0x80u) ? -f2 : f2, wscale * (R)tab[t],
+                                      &Bm[eb & 63u][c0], (eb & 0x80u) ? -f2 : f2, wscale * (R)tab[t + 1], h, gmask);
+            }
+        }
+        for (; t < Lin; ++t) {
+            const unsigned e = sm.tab_f[t];
+            term_any<KH, TPL, R, C2>(sr, si, ar, ai, &Bm[e & 63u][c0], (e & 0x80u) ? -f2 : f2, wscale * (R)tab[t], h, gmask);
+        }
+    } else {
+        term_any<KH, TPL, R, C2>(sr, si, ar, ai, nullptr, R(0), wscale * (R)tab[Lin - 1], h, gmask);
+        int t = Lin - 2;
+        if constexpr (UNR == 2) {
+            for (; t - 1 >= 0; t -= 2) {
+                const unsigned ea = sm.tab_f[t + 1], eb = sm.tab_f[t];
+                term2<KH, TPL, R, C2>(sr, si, ar, ai, &Bm[ea & 63u][c0], (ea & 0x80u) ? f2 : -f2, wscale * (R)tab[t],
+                                      &Bm[eb & 63u][c0], (eb & 0x80u) ? f2 : -f2, wscale * (R)tab[t - 1], h, gmask);
+            }
+        }
+        for (; t >= 0; --t) {
+            const unsigned e = sm.tab_f[t + 1];
+            term_any<KH, TPL, R, C2>(sr, si, ar, ai, &Bm[e & 63u][c0], (e & 0x80u) ? f2 : -f2, wscale * (R)tab[t], h, gmask);
+        }
     }
 }
 
@@ -245,10 +539,63 @@ __device__ __forceinline__ void reduce_to_P(double (&ar)[KH], double (&ai)[KH], 
     __syncthreads();
 }
 
-template <int TPL>
-__device__ __forceinline__ unsigned group_mask() {
-    if constexpr (TPL == 1) return 0u;
-    else return ((1u << TPL) - 1u) << ((threadIdx.x & 31) & ~(TPL - 1));
+// High-digit values of Gray lane hl (plain mixed radix over the high digits), packed 5 bits per digit
+// (radices <= 32), and the lane's weight prod (-1)^v C(M, v) over them.
+static __device__ __forceinline__ uint64_t lane_digits(const Plan& pl, int64_t hl, double* wh_out) {
+    const int hi0 = pl.nin + pl.nmid;
+    uint64_t packed = 0;
+    double wh = 1.0;
+    int64_t rem = hl;
+    for (int i = 0; i < pl.nhi; ++i) {
+        const int R = pl.R[hi0 + i];
+        const int v = (int)(rem % R);
+        rem /= R;
+        if (i < 12) packed |= (uint64_t)v << (5 * i);
+        wh *= signed_binom(pl.M[hi0 + i], v);
+    }
+    *wh_out = wh;
+    return packed;
+}
+
+// Column sums of one lane at a given digit state, FP64: s_j = sum_kd (M_kd - 2 v_kd) B[kd][j] with the
+// inner digits at their start (0) or end (vend) state, the middle digits at middle index pm and the
+// high digits of the lane (packed by lane_digits; more than 12 high digits are decoded from hl).
+template <int KH>
+__device__ __forceinline__ void lane_sums(const Smem& sm, int c0, bool inner_end, int pm, int64_t hl, uint64_t hpack,
+                                          double (&xr)[KH], double (&xi)[KH]) {
+    const Plan& pl = sm.plan;
+#pragma unroll
+    for (int j = 0; j < KH; ++j) { xr[j] = 0.0; xi[j] = 0.0; }
+    const int nin = pl.nin, nmid = pl.nmid, hi0 = nin + nmid, nhi = pl.nhi;
+    auto add = [&](int kd, int v) {
+        const double c = (double)(pl.M[kd] - 2 * v);
+        const double2* b = &sm.B[kd][c0];
+#pragma unroll
+        for (int j = 0; j < KH; ++j) { xr[j] = fma(c, b[j].x, xr[j]); xi[j] = fma(c, b[j].y, xi[j]); }
+    };
+    for (int kd = 0; kd < nin; ++kd) add(kd, inner_end ? sm.plan.vend[kd] : 0);
+    int par = 0;                                       // middle digits top-down (reflected Gray)
+    for (int q = nmid - 1; q >= 0; --q) {
+        const int R = pl.R[nin + q];
+        const int d = (pm / pl.Pmid[q]) % R;
+        const int v = (par & 1) ? R - 1 - d : d;
+        par += v;
+        add(nin + q, v);
+    }
+    int64_t rem = hl;
+    for (int i = 0; i < nhi; ++i) {
+        int v;
+        if (i < 12) {
+            v = (int)((hpack >> (5 * i)) & 31u);
+        } else {
+            int64_t r2 = hl;
+            for (int q = 0; q < i; ++q) r2 /= pl.R[hi0 + q];
+            v = (int)(r2 % pl.R[hi0 + i]);
+        }
+        add(hi0 + i, v);
+    }
+    (void)rem;
+    for (int kd = hi0 + nhi; kd < pl.D; ++kd) add(kd, 0);
 }
 
 // FP64 sweep of tier KP (columns padded to KP: padded column sums hold 1, their B rows are zero).
@@ -256,76 +603,31 @@ template <int KP, int TPL>
 __device__ void sweep_f64(Smem& sm) {
     constexpr int KH = KP / TPL;
     const Plan& pl = sm.plan;
-    const int tid = threadIdx.x, T = blockDim.x;
-    const int lanes = T / TPL, lane = tid / TPL, h = tid % TPL, c0 = h * KH;
+    const int tid = threadIdx.x;
+    const int lanes = blockDim.x / TPL, lane = tid / TPL, h = tid % TPL, c0 = h * KH;
     const unsigned gmask = group_mask<TPL>();
-    const int nin = pl.nin, nmid = pl.nmid, nhi = pl.nhi, D = pl.D, K = pl.K, Lin = pl.Lin;
-    const int64_t Lmid = pl.Lmid, H = pl.H;
+    const int K = pl.K, Lin = pl.Lin, Lmid = pl.Lmid, nin = pl.nin;
+    const int64_t H = pl.H;
     double ar[KH], ai[KH];
 #pragma unroll
     for (int j = 0; j < KH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
     for (int64_t hl = lane; hl < H; hl += lanes) {
-        double sr[KH], si[KH];
-#pragma unroll
-        for (int j = 0; j < KH; ++j) { sr[j] = 0.0; si[j] = 0.0; }
-        double wh = 1.0;
-        int64_t rem = hl;
-        for (int kd = 0; kd < D; ++kd) {
-            int v = 0;
-            if (kd >= nin + nmid && kd < nin + nmid + nhi) {
-                v = (int)(rem % pl.R[kd]);
-                rem /= pl.R[kd];
-                wh *= signed_binom(pl.M[kd], v);
-            }
-            const double c = (double)(pl.M[kd] - 2 * v);
-            const double2* b = &sm.B[kd][c0];
-#pragma unroll
-            for (int j = 0; j < KH; ++j) { sr[j] = fma(c, b[j].x, sr[j]); si[j] = fma(c, b[j].y, si[j]); }
-        }
+        double sr[KH], si[KH], wh;
+        const uint64_t hpack = lane_digits(pl, hl, &wh);
+        lane_sums<KH>(sm, c0, false, 0, hl, hpack, sr, si);
 #pragma unroll
         for (int j = 0; j < KH; ++j) if (c0 + j >= K) { sr[j] = 1.0; si[j] = 0.0; }
-        unsigned char dm[MAXN], vm[MAXN], pp[MAXN];
-        for (int q = 0; q < nmid; ++q) { dm[q] = 0; vm[q] = 0; pp[q] = 0; }
-        double wm = 1.0;
-        for (int64_t pm = 0; pm < Lmid; ++pm) {
+        for (int pm = 0; pm < Lmid; ++pm) {
             if (pm > 0) {
-                int q = 0;
-                while (dm[q] == pl.R[nin + q] - 1) ++q;
-                const int dir = pp[q] ? -1 : 1;
-                for (int mu = 0; mu < q; ++mu) { dm[mu] = 0; pp[mu] ^= 1; }
-                dm[q] += 1;
-                vm[q] = (unsigned char)(vm[q] + dir);
-                const double f = -2.0 * dir;
-                const double2* b = &sm.B[nin + q][c0];
+                const unsigned e = sm.tab_fm[pm];
+                const double f = (e & 0x80u) ? -2.0 : 2.0;
+                const double2* b = &sm.B[nin + (e & 63u)][c0];
 #pragma unroll
                 for (int j = 0; j < KH; ++j) { sr[j] = fma(f, b[j].x, sr[j]); si[j] = fma(f, b[j].y, si[j]); }
-                wm = 1.0;
-                for (int mu = 0; mu < nmid; ++mu) wm *= signed_binom(pl.M[nin + mu], vm[mu]);
             }
-            const double wmh = wh * wm;
-            if (!(pm & 1)) {
-                for (int t = 0; t < Lin; ++t) {
-                    if (t > 0) {
-                        const unsigned e = sm.tab_f[t];
-                        const double f = (e & 0x80u) ? -2.0 : 2.0;
-                        const double2* b = &sm.B[e & 63u][c0];
-#pragma unroll
-                        for (int j = 0; j < KH; ++j) { sr[j] = fma(f, b[j].x, sr[j]); si[j] = fma(f, b[j].y, si[j]); }
-                    }
-                    allbutone_acc<KH, TPL, double>(sr, si, wmh * sm.tab_w[t], ar, ai, h, gmask);
-                }
-            } else {
-                for (int t = Lin - 1; t >= 0; --t) {
-                    if (t < Lin - 1) {
-                        const unsigned e = sm.tab_f[t + 1];
-                        const double f = (e & 0x80u) ? 2.0 : -2.0;
-                        const double2* b = &sm.B[e & 63u][c0];
-#pragma unroll
-                        for (int j = 0; j < KH; ++j) { sr[j] = fma(f, b[j].x, sr[j]); si[j] = fma(f, b[j].y, si[j]); }
-                    }
-                    allbutone_acc<KH, TPL, double>(sr, si, wmh * sm.tab_w[t], ar, ai, h, gmask);
-                }
-            }
+            const double wmh = wh * sm.tab_wm[pm];
+            inner_block<KH, TPL, PE_UNROLL, double, double2, double>(sr, si, ar, ai, sm, sm.B, sm.tab_w, wmh, 2.0,
+                                                                    !(pm & 1), Lin, c0, h, gmask);
         }
     }
     reduce_to_P<KH, TPL>(ar, ai, sm, c0);
@@ -337,57 +639,23 @@ template <int KP, int TPL>
 __device__ void sweep_mixed(Smem& sm) {
     constexpr int KH = KP / TPL;
     const Plan& pl = sm.plan;
-    const int tid = threadIdx.x, T = blockDim.x;
-    const int lanes = T / TPL, lane = tid / TPL, h = tid % TPL, c0 = h * KH;
+    const int tid = threadIdx.x;
+    const int lanes = blockDim.x / TPL, lane = tid / TPL, h = tid % TPL, c0 = h * KH;
     const unsigned gmask = group_mask<TPL>();
-    const int nin = pl.nin, nmid = pl.nmid, nhi = pl.nhi, D = pl.D, K = pl.K, Lin = pl.Lin;
-    const int64_t Lmid = pl.Lmid, H = pl.H;
+    const int K = pl.K, Lin = pl.Lin, Lmid = pl.Lmid;
+    const int64_t H = pl.H;
     double ar[KH], ai[KH];
 #pragma unroll
     for (int j = 0; j < KH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
     for (int64_t hl = lane; hl < H; hl += lanes) {
-        unsigned char vh[MAXN];
-        double wh = 1.0;
-        {
-            int64_t rem = hl;
-            for (int i = 0; i < nhi; ++i) {
-                const int kd = nin + nmid + i;
-                const int v = (int)(rem % pl.R[kd]);
-                rem /= pl.R[kd];
-                vh[i] = (unsigned char)v;
-                wh *= signed_binom(pl.M[kd], v);
-            }
-        }
-        unsigned char dm[MAXN], vm[MAXN], pp[MAXN];
-        for (int q = 0; q < nmid; ++q) { dm[q] = 0; vm[q] = 0; pp[q] = 0; }
-        double wm = 1.0;
-        for (int64_t pm = 0; pm < Lmid; ++pm) {
-            if (pm > 0) {
-                int q = 0;
-                while (dm[q] == pl.R[nin + q] - 1) ++q;
-                const int dir = pp[q] ? -1 : 1;
-                for (int mu = 0; mu < q; ++mu) { dm[mu] = 0; pp[mu] ^= 1; }
-                dm[q] += 1;
-                vm[q] = (unsigned char)(vm[q] + dir);
-                wm = 1.0;
-                for (int mu = 0; mu < nmid; ++mu) wm *= signed_binom(pl.M[nin + mu], vm[mu]);
-            }
+        double wh;
+        const uint64_t hpack = lane_digits(pl, hl, &wh);
+        for (int pm = 0; pm < Lmid; ++pm) {
             const bool fwd = !(pm & 1);
             float sr[KH], si[KH];
             {
                 double xr[KH], xi[KH];
-#pragma unroll
-                for (int j = 0; j < KH; ++j) { xr[j] = 0.0; xi[j] = 0.0; }
-                for (int kd = 0; kd < D; ++kd) {
-                    int v = 0;
-                    if (kd < nin) v = fwd ? 0 : sm.plan.vend[kd];
-                    else if (kd < nin + nmid) v = vm[kd - nin];
-                    else if (kd < nin + nmid + nhi) v = vh[kd - nin - nmid];
-                    const double c = (double)(pl.M[kd] - 2 * v);
-                    const double2* b = &sm.B[kd][c0];
-#pragma unroll
-                    for (int j = 0; j < KH; ++j) { xr[j] = fma(c, b[j].x, xr[j]); xi[j] = fma(c, b[j].y, xi[j]); }
-                }
+                lane_sums<KH>(sm, c0, !fwd, pm, hl, hpack, xr, xi);
 #pragma unroll
                 for (int j = 0; j < KH; ++j) {
                     const bool pad = c0 + j >= K;
@@ -398,30 +666,9 @@ __device__ void sweep_mixed(Smem& sm) {
             float a32r[KH], a32i[KH];
 #pragma unroll
             for (int j = 0; j < KH; ++j) { a32r[j] = 0.0f; a32i[j] = 0.0f; }
-            if (fwd) {
-                for (int t = 0; t < Lin; ++t) {
-                    if (t > 0) {
-                        const unsigned e = sm.tab_f[t];
-                        const float f = (e & 0x80u) ? -1.0f : 1.0f;
-                        const float2* b = &sm.B32[e & 63u][c0];
-#pragma unroll
-                        for (int j = 0; j < KH; ++j) { sr[j] = fmaf(f, b[j].x, sr[j]); si[j] = fmaf(f, b[j].y, si[j]); }
-                    }
-                    allbutone_acc<KH, TPL, float>(sr, si, sm.tab_w32[t], a32r, a32i, h, gmask);
-                }
-            } else {
-                for (int t = Lin - 1; t >= 0; --t) {
-                    if (t < Lin - 1) {
-                        const unsigned e = sm.tab_f[t + 1];
-                        const float f = (e & 0x80u) ? 1.0f : -1.0f;
-                        const float2* b = &sm.B32[e & 63u][c0];
-#pragma unroll
-                        for (int j = 0; j < KH; ++j) { sr[j] = fmaf(f, b[j].x, sr[j]); si[j] = fmaf(f, b[j].y, si[j]); }
-                    }
-                    allbutone_acc<KH, TPL, float>(sr, si, sm.tab_w32[t], a32r, a32i, h, gmask);
-                }
-            }
-            const double wmh = wh * wm;
+            inner_block<KH, TPL, PE_UNROLL, float, float2, float>(sr, si, a32r, a32i, sm, sm.B32, sm.tab_w32, 1.0f, 1.0f,
+                                                                 fwd, Lin, c0, h, gmask);
+            const double wmh = wh * sm.tab_wm[pm];
 #pragma unroll
             for (int j = 0; j < KH; ++j) { ar[j] = fma(wmh, (double)a32r[j], ar[j]); ai[j] = fma(wmh, (double)a32i[j], ai[j]); }
         }
@@ -458,12 +705,24 @@ __device__ void dispatch_mixed(Smem& sm, int K) {
     PE_TIER(32, (sweep_mixed<32, TPL>(sm)))
 }
 
+// One cofactor step of the stream held in shared memory (K1 >= 1): plan, prepare, sweep.
+template <int TPL, int KPM, bool MIXED>
+__device__ __forceinline__ void cofactor_step(Smem& sm, const double2* A, int64_t rs, int64_t cs, int K1, int K) {
+    if (threadIdx.x < 32) plan_step(sm, K1, K, blockDim.x / TPL, MIXED ? MIXED_LIN : LIN_MAX);
+    __syncthreads();
+    prepare_step(sm, A, rs, cs, MIXED);
+    __syncthreads();
+    if constexpr (MIXED) dispatch_mixed<TPL, KPM>(sm, K);
+    else dispatch_f64<TPL, KPM>(sm, K);
+}
+
 // ---------------------------------------------------------------------------------------- draw
 // Marginal over the m output modes, FP64 block scan (contiguous chunk per thread, warp scan, warps
 // in order), then idx = min(#{rho : cw_rho < u * tot}, m - 1) with tot = cw[m - 1]
-// (cofactors_triton.py:298-308).  Returns the gap min |cw - u tot| / tot through sm.fmin[0].
+// (cofactors_triton.py:298-308).  Thread 0 records the pick and updates the groups; the gap
+// min |cw - u tot| / tot is left in sm.fmin[0].
 static __device__ void draw_step(Smem& sm, double* __restrict__ wgt, const double2* __restrict__ A, int64_t rs, int64_t cs,
-                          int m, int k, double u, double* __restrict__ marg_row) {
+                                 int m, int k, double u, double* __restrict__ marg_row, bool update_groups) {
     const int tid = threadIdx.x, T = blockDim.x, lid = tid & 31, wid = tid >> 5, nw = T >> 5;
     for (int rho = tid; rho < m; rho += T) {
         double xr = 0.0, xi = 0.0;
@@ -525,8 +784,10 @@ static __device__ void draw_step(Smem& sm, double* __restrict__ wgt, const doubl
         int c = 0;
         double g = 1.0e300;
         for (int w = 0; w < nw; ++w) { c += sm.cnt[w]; g = fmin(g, sm.fmin[w]); }
-        sm.rows[k - 1] = min(c, m - 1);
+        const int pick = min(c, m - 1);
+        sm.rows[k - 1] = pick;
         sm.fmin[0] = g / tot;
+        if (update_groups) add_to_groups(sm, pick);
     }
     __syncthreads();
 }
@@ -548,6 +809,7 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
         else sm.cols[tid] = (int)c;
     }
     if (!ok && tid == 0) sm.bad = 1;
+    if (tid == 0) sm.ngrp = 0;
     __syncthreads();
     if (sm.bad) {
         if (tid == 0) record_error(p.status, p.detail, s);
@@ -560,12 +822,7 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
             if (tid == 0) sm.P[0] = make_double2(1.0, 0.0);
             __syncthreads();
         } else {
-            if (tid == 0) plan_step(sm.plan, sm.rows, K1, K, blockDim.x / TPL);
-            __syncthreads();
-            prepare_step(sm, A, 1, m, MIXED);
-            __syncthreads();
-            if constexpr (MIXED) dispatch_mixed<TPL, KPM>(sm, K);
-            else dispatch_f64<TPL, KPM>(sm, K);
+            cofactor_step<TPL, KPM, MIXED>(sm, A, 1, m, K1, K);
         }
         double u;
         if (p.uniforms) {
@@ -576,12 +833,16 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
             u = chain_uniform((uint64_t)p.seeds[row * p.n_stride + (k - 1)], ro);
         }
         double* mrow = p.marg ? p.marg + ((size_t)s * p.n_stride + (k - 1)) * p.marg_stride : nullptr;
-        draw_step(sm, wgt, A, 1, m, m, k, u, mrow);
         if constexpr (MIXED) {
+            draw_step(sm, wgt, A, 1, m, m, k, u, mrow, false);
             if (K1 > 0 && sm.fmin[0] <= p.tau) {          // uniform: read after the draw's final barrier
                 dispatch_f64<4, KPM>(sm, K);
-                draw_step(sm, wgt, A, 1, m, m, k, u, mrow);
+                draw_step(sm, wgt, A, 1, m, m, k, u, mrow, false);
             }
+            if (tid == 0) add_to_groups(sm, sm.rows[k - 1]);
+            __syncthreads();
+        } else {
+            draw_step(sm, wgt, A, 1, m, m, k, u, mrow, true);
         }
     }
     for (int j = tid; j < nk; j += blockDim.x) p.rows[s * p.n_stride + j] = sm.rows[j];
@@ -597,7 +858,7 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
 __host__ __device__ constexpr size_t smem_fixed_bytes() { return (sizeof(Smem) + 15) & ~(size_t)15; }
 
 template <int TPL, int KPM, bool MIXED>
-__global__ void __launch_bounds__(256) fock_chain_kernel(ChainParams p) {
+__global__ void __launch_bounds__(256, PE_MINB) fock_chain_kernel(ChainParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
     double* wgt = reinterpret_cast<double*>(smem_raw + smem_fixed_bytes());
@@ -629,7 +890,7 @@ __global__ void __launch_bounds__(256) cofactor_kernel(const double2* __restrict
     Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
     const int tid = threadIdx.x;
     for (int64_t s = blockIdx.x; s < S; s += gridDim.x) {
-        if (tid == 0) sm.bad = 0;
+        if (tid == 0) { sm.bad = 0; sm.ngrp = 0; }
         __syncthreads();
         if (tid < K) sm.cols[tid] = tid;
         if (tid < K - 1) {
@@ -643,16 +904,13 @@ __global__ void __launch_bounds__(256) cofactor_kernel(const double2* __restrict
             __syncthreads();
             continue;
         }
+        if (tid == 0) for (int i = 0; i < K - 1; ++i) add_to_groups(sm, sm.rows[i]);
+        __syncthreads();
         if (K == 1) {
             if (tid == 0) sm.P[0] = make_double2(1.0, 0.0);
             __syncthreads();
         } else {
-            if (tid == 0) plan_step(sm.plan, sm.rows, K - 1, K, blockDim.x / TPL);
-            __syncthreads();
-            prepare_step(sm, A + s * (int64_t)m * K, K, 1, MIXED);
-            __syncthreads();
-            if constexpr (MIXED) dispatch_mixed<TPL, KPM>(sm, K);
-            else dispatch_f64<TPL, KPM>(sm, K);
+            cofactor_step<TPL, KPM, MIXED>(sm, A + s * (int64_t)m * K, K, 1, K - 1, K);
         }
         if (tid < K) P[s * K + tid] = sm.P[tid];
         __syncthreads();

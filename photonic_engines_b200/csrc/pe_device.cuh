@@ -1,5 +1,5 @@
-// Device building blocks of the Fock chain kernels: Philox uniforms, exact signed binomials, complex
-// helpers and the per-CTA shared-memory layout.  sm_100a only.
+// Device building blocks of the Fock chain kernels: Philox uniforms, exact signed binomials and the
+// per-CTA shared-memory layout.  sm_100a only.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -7,7 +7,8 @@
 namespace pe {
 
 constexpr int MAXN = 32;        // photons per stream = largest cofactor tier (columns)
-constexpr int LIN_MAX = 512;    // inner Gray block: terms enumerated from the shared schedule table
+constexpr int LIN_MAX = 512;    // inner Gray block: terms walked from the shared inner schedule
+constexpr int MID_MAX = 1024;   // middle Gray block: inner blocks walked from the shared middle schedule
 constexpr int MAX_WARPS = 8;    // CTA of at most 256 threads
 
 // ------------------------------------------------------------------------------------------ RNG
@@ -54,23 +55,27 @@ static __device__ __forceinline__ double signed_binom(int M, int v) {
 }
 
 // ------------------------------------------------------------------------------------------ layout
-// Per-step plan of one stream, written by thread 0.  Kernel digits are ordered
-//   [inner: nin | middle: nmid | high: nhi | fixed: nfix]
-// inner digits are walked from the shared schedule table (one CTA-uniform transition per term),
-// middle digits by an odometer once per inner block, high digits index the Gray lanes, fixed
-// digits have radix 1 (their sign never changes).
+// Per-step plan of one stream.  The collapsed sum runs over v in prod_d {0..R_d - 1}; its digits are
+// ordered for the kernel as
+//   [inner: nin | middle: nmid | high: nhi | fixed]
+// inner digits are walked from the shared inner schedule (one CTA-uniform transition per term),
+// middle digits from the shared middle schedule once per inner block, high digits index the Gray
+// lanes (each lane owns one combination of them), fixed digits have radix 1.
 struct Plan {
     int64_t N;          // terms of the collapsed sum (the reference's addend count)
     int64_t H;          // lanes = product of high radices
-    int64_t Lmid;       // middle combinations per lane
-    int Lin;            // inner combinations per block (<= LIN_MAX)
+    int Lin, Lmid;      // inner / middle combinations
     int K, K1, D;       // columns, chosen rows, digits (distinct chosen rows)
     int nin, nmid, nhi;
-    double scale;       // 2^-K1, doubled when the top digit is halved
+    double scale;       // 2^-K1, doubled when an odd group is halved
     int R[MAXN];        // radix per kernel digit
     int M[MAXN];        // multiplicity per kernel digit
     int drow[MAXN];     // output mode per kernel digit
+    int Pin[MAXN];      // prefix products of the inner radices
+    int Pmid[MAXN];     // prefix products of the middle radices
     unsigned char vend[MAXN];   // inner digit values after a forward inner block
+    int sortR[MAXN];    // scratch of the planner: active digits by ascending radix
+    int sortG[MAXN];
 };
 
 struct Smem {
@@ -80,17 +85,21 @@ struct Smem {
     float2 B32[MAXN][MAXN];        // 2 * B in float32 (the mixed form's Gray update)
     double tab_w[LIN_MAX];         // inner weight prod (-1)^v C(M, v) at inner index t
     float tab_w32[LIN_MAX];
-    unsigned char tab_f[LIN_MAX];  // transition into t: digit | 0x80 when the update is -2 b
+    double tab_wm[MID_MAX];        // middle weight at middle index
+    unsigned char tab_f[LIN_MAX];  // transition into inner index t: digit | 0x80 when the update is -2 b
+    unsigned char tab_fm[MID_MAX]; // transition into middle index: middle digit | 0x80 when -2 b
     double2 red[MAX_WARPS][MAXN];  // cross-warp reduction
     double scan[MAX_WARPS];
     double fmin[MAX_WARPS];
     int cnt[MAX_WARPS];
     int rows[MAXN];                // chosen modes so far
     int cols[MAXN];                // input columns of the stream in chain order
+    int grow[MAXN];                // distinct chosen modes (groups), in order of first appearance
+    int gmul[MAXN];                // their multiplicities
+    int ngrp;
     int64_t cur;                   // stream being processed (-1: queue drained)
-    double tot, target, u;
+    double tot, target;
     int bad;                       // set by any thread that saw an out-of-range index
-    int refine;                    // mixed form: the draw fell inside the guard band
 };
 
 }  // namespace pe
