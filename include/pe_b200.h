@@ -84,6 +84,29 @@ int pe_fock_chain(int precision, const double* d_acol, const int64_t* d_inst_off
                   int grid_ctas, void* stream);
 
 /*
+ * pe_fock_chain without a workspace argument: the same chains and outputs, for callers that cannot
+ * allocate device memory when they sample (a host callback or other context where CUDA allocation is not
+ * allowed, a serving process whose device memory all belongs to its own arena, a foreign-language
+ * binding that can pass buffers but cannot call cudaMalloc).  No counterpart in the reference.
+ *
+ * Its scratch (the work-queue counter and the status word) lives in a static device array of 4096
+ * bytes that every GPU loading this library holds until exit; a requirement above that size is
+ * rejected with PE_ERR_SIZE.  The first call on a device looks the array up with cudaGetSymbolAddress
+ * (once per device): make that first call before any stream capture.  The call allocates nothing: no
+ * cudaMalloc, no cudaFree.  All calls share the array and it keeps the last call's contents; each call
+ * clears the queue counter and status word on its stream before its launch, and calls whose kernels
+ * overlap on the GPU race on it.  d_status (optional, device int) receives the device status word
+ * (0, or PE_ERR_DEVICE after an out-of-range index).  Other arguments as pe_fock_chain.
+ */
+int pe_fock_chain_noalloc(int precision, const double* d_acol, const int64_t* d_inst_off,
+                          const int32_t* d_inst_m, const int32_t* d_inst_n, int G, int m_max, int64_t S,
+                          const int64_t* d_dp, const int32_t* d_nk, const int64_t* d_cols, int n_stride,
+                          const double* d_uniforms, const int64_t* d_seeds, const int64_t* d_seed_row,
+                          const int64_t* d_rng_off, const int64_t* d_order, int64_t* d_rows, int64_t* d_occ,
+                          int occ_stride, double* d_marg, int marg_stride, int* d_status, int block_threads,
+                          int tpl, int grid_ctas, void* stream);
+
+/*
  * Laplace cofactors P[s, c] = per(A_s[rows_s, all columns but c]) of S blocks, the reference's
  * 2020 kernel entry point:
  *   photonic_engines/clifford/cofactors_triton.py:509-530  laplace_cofactors_rows

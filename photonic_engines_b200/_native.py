@@ -47,6 +47,9 @@ def load() -> ctypes.CDLL:
     L.pe_fock_chain.restype = _i32
     L.pe_fock_chain.argtypes = [_i32, _vp, _vp, _vp, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp,
                                 _vp, _vp, _vp, _i32, _vp, _i32, _vp, ctypes.c_size_t, _i32, _i32, _i32, _vp]
+    L.pe_fock_chain_noalloc.restype = _i32
+    L.pe_fock_chain_noalloc.argtypes = [_i32, _vp, _vp, _vp, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i32, _vp, _vp, _vp,
+                                        _vp, _vp, _vp, _vp, _i32, _vp, _i32, _vp, _i32, _i32, _i32, _vp]
     L.pe_cofactors_rows.restype = _i32
     L.pe_cofactors_rows.argtypes = [_i32, _vp, _vp, _i64, _i32, _i32, _vp, _vp, ctypes.c_size_t, _i32, _i32, _vp]
     L.pe_pipe_probe.restype = _i32
@@ -60,8 +63,8 @@ def load() -> ctypes.CDLL:
 
 
 # every symbol the C header declares (checked by the CPU test that loads the library)
-EXPORTED = ("pe_version", "pe_max_modes", "pe_chain_workspace_bytes", "pe_fock_chain", "pe_cofactors_rows",
-            "pe_pipe_probe", "pe_read_status", "pe_status_string")
+EXPORTED = ("pe_version", "pe_max_modes", "pe_chain_workspace_bytes", "pe_fock_chain", "pe_fock_chain_noalloc",
+            "pe_cofactors_rows", "pe_pipe_probe", "pe_read_status", "pe_status_string")
 
 
 def check(rc: int, what: str) -> None:

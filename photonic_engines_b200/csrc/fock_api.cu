@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "fock_kernels.cuh"
 #include "fock_registry.h"
 
@@ -221,5 +223,62 @@ extern "C" int pe_pipe_probe(int precision, int iters, void* d_out, size_t out_b
         pipe_probe_kernel<float><<<blocks, threads, 0, st>>>((float*)d_out, 0.999999f, 1e-7f, iters);
     if (cudaGetLastError() != cudaSuccess) return PE_ERR_CUDA;
     *flops = 2.0 * 8.0 * (double)iters * (double)blocks * (double)threads;
+    return PE_OK;
+}
+
+// ---------------------------------------------------------------------------------------- allocation-free chain
+// For callers that cannot allocate device memory themselves at the time they sample: code running in a
+// host callback or another context where CUDA allocation calls are not allowed, a serving process whose
+// device memory is all handed out by its own arena, or a foreign-language binding that can pass the
+// buffers it was given but has no way to call cudaMalloc.  pe_fock_chain needs a small caller-provided
+// workspace (the work-queue counter and the status word); this entry point keeps that scratch in a
+// static device array instead, so the caller passes inputs and outputs only.
+//
+// The array is PE_NOALLOC_SCRATCH_BYTES long; every GPU that loads this library holds it until the
+// process exits.  All calls share it and it keeps the last call's contents: each call clears the part
+// that must start at zero (queue counter, status word) on its stream before launching, and calls whose
+// kernels overlap on the GPU (different streams, or different host threads on one device) race on it.
+constexpr size_t PE_NOALLOC_SCRATCH_BYTES = 4096;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PE_NOALLOC_SCRATCH_BYTES];
+
+constexpr int PE_NOALLOC_MAX_DEVICES = 64;
+static void* g_noalloc_ptr[PE_NOALLOC_MAX_DEVICES];
+static std::mutex g_noalloc_mutex;
+
+// Device address of the scratch on the current device.  The host-side name of the array is only a
+// stand-in; the address comes from cudaGetSymbolAddress, once per device, with that device current.
+static int noalloc_scratch(void** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PE_ERR_CUDA;
+    if (dev < 0 || dev >= PE_NOALLOC_MAX_DEVICES) return PE_ERR_SIZE;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return PE_ERR_CUDA;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return PE_OK;
+}
+
+extern "C" int pe_fock_chain_noalloc(int precision, const double* d_acol, const int64_t* d_inst_off,
+                                     const int32_t* d_inst_m, const int32_t* d_inst_n, int G, int m_max, int64_t S,
+                                     const int64_t* d_dp, const int32_t* d_nk, const int64_t* d_cols, int n_stride,
+                                     const double* d_uniforms, const int64_t* d_seeds, const int64_t* d_seed_row,
+                                     const int64_t* d_rng_off, const int64_t* d_order, int64_t* d_rows, int64_t* d_occ,
+                                     int occ_stride, double* d_marg, int marg_stride, int* d_status,
+                                     int block_threads, int tpl, int grid_ctas, void* stream) {
+    if (pe_chain_workspace_bytes(S) > PE_NOALLOC_SCRATCH_BYTES) return PE_ERR_SIZE;
+    void* scratch = nullptr;
+    const int rc0 = noalloc_scratch(&scratch);
+    if (rc0 != PE_OK) return rc0;
+    const int rc = pe_fock_chain(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, d_nk, d_cols,
+                                 n_stride, d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ,
+                                 occ_stride, d_marg, marg_stride, scratch, PE_NOALLOC_SCRATCH_BYTES, block_threads, tpl,
+                                 grid_ctas, stream);
+    if (rc != PE_OK) return rc;
+    if (d_status && cudaMemcpyAsync(d_status, (const char*)scratch + 8, sizeof(int), cudaMemcpyDeviceToDevice,
+                                    (cudaStream_t)stream) != cudaSuccess)
+        return PE_ERR_CUDA;
     return PE_OK;
 }
