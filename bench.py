@@ -310,6 +310,28 @@ def cpu_baseline(S: int) -> dict:
             "sample": f"{S} chains of the n=20 m=400 workload, oracle/ C port, {threads} threads, {dt:.1f} s"}
 
 
+def profile_launch(precision: str):
+    """One warm-up launch and one launch of the chain kernel on the benchmark workload (for ncu -s 1 -c 1)."""
+    import torch
+
+    from photonic_engines_b200.clifford.kernels import chain, pack_instances
+    dev = torch.device("cuda")
+    g = torch.Generator().manual_seed(USEED)
+    z = torch.randn(M_MODES, M_MODES, generator=g, dtype=torch.float64) + 1j * torch.randn(
+        M_MODES, M_MODES, generator=g, dtype=torch.float64)
+    q, r = torch.linalg.qr(z)
+    d = torch.diagonal(r)
+    U = (q * (d / d.abs()).unsqueeze(0)).to(dev)
+    acol, off, mm, nn = pack_instances(U, list(range(N_PHOT)))
+    gen = torch.Generator(device=dev).manual_seed(5)
+    for _ in range(2):
+        sig = torch.argsort(torch.rand(SHOTS, N_PHOT, generator=gen, device=dev), dim=1)
+        seeds = torch.randint(0, 2 ** 31 - 1, (N_PHOT,), generator=gen, device=dev)
+        chain(acol, off, mm, nn, torch.zeros(SHOTS, dtype=torch.int64, device=dev), sig, m_max=M_MODES, seeds=seeds,
+              precision=precision)
+    torch.cuda.synchronize()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -318,7 +340,12 @@ def main():
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--ref-shots", type=int, default=0, help="chains per CPU sample (0: scaled to the cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-launch", choices=("f64", "mixed"), default=None,
+                    help="run only two chain launches of the workload (a target for ncu -s 1 -c 1)")
     args = ap.parse_args()
+    if args.profile_launch:
+        profile_launch(args.profile_launch)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
