@@ -117,6 +117,28 @@ int pe_cofactors_rows(int precision, const double* d_a, const int64_t* d_rows, i
                       double* d_p, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
                       void* stream);
 
+/*
+ * Device-side partition of S shots into chains (batched form): per photon of shot s (instance dp[s],
+ * inst_n[g] photons), lost with probability 1 - eta[g], else interfering with probability x[g] (x-model;
+ * x >= 1: always), else alone.  Slot 0 of a shot holds its interfering photons in a uniformly random
+ * order (d_nk = their count); with `singles` = 1, slots 1..n_stride hold one lone photon each (nk 0 or
+ * 1).  Chain c = s * slots + q; d_cols [C][n_stride], d_nk [C], d_chain_dp [C] (instance), d_out_row [C]
+ * (= s).  Draws: Philox4x32-10 keyed by the device int64 *d_key (graph-capturable).  The law of
+ *   photonic_engines/imperfections.py:529-590   draw_roles / partition / route_classical
+ *   photonic_engines/clifford/sampler.py:183-215 grouping by surviving columns, one pass per count
+ * without host work; the draws differ from the reference's host draws (fock_sample keeps those).
+ */
+int pe_partition_shots(const int64_t* d_dp, const int32_t* d_inst_n, const double* d_eta, const double* d_x,
+                       int64_t S, int n_stride, int singles, const int64_t* d_key, int64_t* d_cols, int32_t* d_nk,
+                       int64_t* d_chain_dp, int64_t* d_out_row, int* d_status, void* stream);
+
+/*
+ * Occupations [S][occ_stride] from chains: zeroed, then occ[out_row[c]][rows[c][j]] += 1 for j < nk[c]
+ * (photonic_engines/clifford/sampler.py:172, :214).  Index errors set *d_status to PE_ERR_DEVICE.
+ */
+int pe_scatter_occupations(const int64_t* d_rows, const int32_t* d_nk, const int64_t* d_out_row, int64_t C,
+                           int n_stride, int64_t* d_occ, int occ_stride, int64_t S, int* d_status, void* stream);
+
 /* Arithmetic-pipe probe (no counterpart in the reference: a measurement aid).  Launches 8 independent
  * FMA chains per thread, `iters` rounds, on (SMs x 8) CTAs of 256 threads, in FP64
  * (PE_PRECISION_F64) or FP32 (PE_PRECISION_MIXED); *flops receives the FLOPs the launch performs

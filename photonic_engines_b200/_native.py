@@ -52,6 +52,10 @@ def load() -> ctypes.CDLL:
                                         _vp, _vp, _vp, _vp, _i32, _vp, _i32, _vp, _i32, _i32, _i32, _vp]
     L.pe_cofactors_rows.restype = _i32
     L.pe_cofactors_rows.argtypes = [_i32, _vp, _vp, _i64, _i32, _i32, _vp, _vp, ctypes.c_size_t, _i32, _i32, _vp]
+    L.pe_partition_shots.restype = _i32
+    L.pe_partition_shots.argtypes = [_vp, _vp, _vp, _vp, _i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.pe_scatter_occupations.restype = _i32
+    L.pe_scatter_occupations.argtypes = [_vp, _vp, _vp, _i64, _i32, _vp, _i32, _i64, _vp, _vp]
     L.pe_pipe_probe.restype = _i32
     L.pe_pipe_probe.argtypes = [_i32, _i32, _vp, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double), _vp]
     L.pe_read_status.restype = _i32
@@ -64,7 +68,8 @@ def load() -> ctypes.CDLL:
 
 # every symbol the C header declares (checked by the CPU test that loads the library)
 EXPORTED = ("pe_version", "pe_max_modes", "pe_chain_workspace_bytes", "pe_fock_chain", "pe_fock_chain_noalloc",
-            "pe_cofactors_rows", "pe_pipe_probe", "pe_read_status", "pe_status_string")
+            "pe_cofactors_rows", "pe_partition_shots", "pe_scatter_occupations", "pe_pipe_probe", "pe_read_status",
+            "pe_status_string")
 
 
 def check(rc: int, what: str) -> None:

@@ -1,0 +1,87 @@
+"""Launch-shape autotuner for the chain kernel.
+
+Candidates are (threads per Gray lane, CTA threads).  `tune` times each candidate on the caller's actual
+workload (a callable running one launch with that shape), keeps the fastest, and caches the choice in a
+JSON file keyed by the GPU name, the precision and a workload key, so later processes reuse it.  The cache
+lives at $PE_TUNE_CACHE (default ~/.cache/photonic_engines_b200/tune.json).
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import torch
+
+CANDIDATES = {8: [(1, 128), (1, 256), (2, 128), (2, 256)],
+              16: [(1, 128), (2, 128), (2, 256), (4, 256)],
+              20: [(2, 128), (2, 256), (4, 128), (4, 256)],
+              24: [(2, 128), (2, 256), (4, 128), (4, 256)],
+              28: [(2, 256), (4, 128), (4, 256)],
+              32: [(2, 256), (4, 128), (4, 256)]}
+
+
+def _cache_path() -> str:
+    return os.environ.get("PE_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "photonic_engines_b200",
+                                                        "tune.json"))
+
+
+def _load() -> dict:
+    try:
+        with open(_cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(cache: dict) -> None:
+    path = _cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+
+
+def tier(n: int) -> int:
+    for k in sorted(CANDIDATES):
+        if n <= k:
+            return k
+    raise ValueError(f"at most 32 photons (got {n})")
+
+
+def key(device, precision: str, workload: str) -> str:
+    return f"{torch.cuda.get_device_name(device)}|{precision}|{workload}"
+
+
+def lookup(device, precision: str, workload: str):
+    hit = _load().get(key(device, precision, workload))
+    return tuple(hit) if hit else None
+
+
+def tune(run, device, precision: str, n_tier: int, workload: str, reps: int = 2, force: bool = False):
+    """run(tpl, block) performs one launch on the current stream.  Returns the fastest (tpl, block)."""
+    k = key(device, precision, workload)
+    cache = _load()
+    if not force and k in cache:
+        return tuple(cache[k])
+    best, best_ms = None, float("inf")
+    for tpl, block in CANDIDATES[n_tier]:
+        run(tpl, block)                                         # warm-up (module load, attribute set-up)
+        times = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run(tpl, block)
+            e1.record()
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ms = min(times)
+        if ms < best_ms:
+            best, best_ms = (tpl, block), ms
+    cache = _load()
+    cache[k] = list(best)
+    _store(cache)
+    return best

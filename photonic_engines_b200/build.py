@@ -59,10 +59,13 @@ def build(jobs: int | None = None, verbose: bool = False, ptxas_info: bool = Fal
         if _stale(obj, deps):
             tasks.append([NVCC, *ARCH, *FLAGS, *(["-Xptxas", "-v"] if ptxas_info else []), f"-DPE_MIXED={mx}",
                           f"-DPE_TPL={tpl}", f"-DPE_KPM={kpm}", "-c", os.path.join(CSRC, "fock_inst.cu"), "-o", obj])
-    api_obj = os.path.join(OBJ, "fock_api.o")
-    if _stale(api_obj, deps):
-        tasks.append([NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, "fock_api.cu"), "-o", api_obj])
-    objs = [os.path.join(OBJ, f"fock_m{mx}_t{tpl}_k{kpm}.o") for mx, tpl, kpm in VARIANTS] + [api_obj]
+    extra = []
+    for name in ("fock_api", "fock_batch"):
+        obj = os.path.join(OBJ, f"{name}.o")
+        extra.append(obj)
+        if _stale(obj, deps):
+            tasks.append([NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, f"{name}.cu"), "-o", obj])
+    objs = [os.path.join(OBJ, f"fock_m{mx}_t{tpl}_k{kpm}.o") for mx, tpl, kpm in VARIANTS] + extra
     if tasks:
         with ThreadPoolExecutor(jobs or os.cpu_count() or 4) as ex:
             for out in ex.map(_run, tasks):

@@ -3,6 +3,7 @@
     fock_sample(U, in_modes, shots, generator, loss=, indist=, ...)   the reference's entry point
     sample(FockState, U, shots, generator, ...)                        dispatch on the input state
     sample_chains(U, in_modes, sigma, uniforms=...)                     chains with a given column order
+    BatchedSampler(circuits, shots, loss=, indist=)                     many circuits, one launch, CUDA graph
     laplace_cofactors_rows(A, rows)                                     the cofactor step alone
 
 Mirrors photonic_engines/clifford/__init__.py:139-166 for Fock inputs; other input types (emitter,
@@ -13,10 +14,11 @@ from __future__ import annotations
 import torch
 
 from ..states import FockState
+from .batch import BatchedSampler
 from .kernels import laplace_cofactors_rows
 from .sampler import fock_sample, sample_chains
 
-__all__ = ["fock_sample", "laplace_cofactors_rows", "sample", "sample_chains"]
+__all__ = ["BatchedSampler", "fock_sample", "laplace_cofactors_rows", "sample", "sample_chains"]
 
 
 def sample(state, U: torch.Tensor, shots: int, generator: torch.Generator | None = None, **kw):

@@ -1,0 +1,186 @@
+"""Batched sampler: many independent circuits (different m and n), lossy and partially distinguishable
+shots, in ONE persistent chain launch, replayed as a captured CUDA graph.
+
+    bs = BatchedSampler([(U_0, modes_0), (U_1, modes_1), ...], shots=1000, loss=[0.8, 0.9, ...],
+                        indist=None, precision="mixed", seed=0)
+    occ = bs.sample()                  # [S_total, m_max] int64; rows of circuit g are bs.rows_of(g)
+
+One replay is: fresh Philox key and per-step seeds from the device generator, the device-side partition
+of every shot into chains (`pe_partition_shots`: lost photons dropped, interfering photons in a uniform
+random order, lone photons as one-photon chains), longest chains first, the chain kernel over all chains,
+and the occupations (`pe_scatter_occupations`).  No host work and no host synchronisation per batch.
+The law is the reference's (lossy / x-model partially distinguishable Fock sampling); the draws are not
+the reference's host draws — `fock_sample` is the path that reproduces those.  The reference's
+equivalent is one `fock_sample(..., loss=eta_g)` call per circuit.
+"""
+from __future__ import annotations
+
+import torch
+
+from .. import _native as N
+from .. import autotune
+from .kernels import pack_ragged
+
+
+def _per_instance(v, G, default):
+    if v is None:
+        return [default] * G
+    if isinstance(v, (list, tuple)):
+        if len(v) != G:
+            raise ValueError(f"one value per circuit ({G}) expected, got {len(v)}")
+        return [default if x is None else float(x) for x in v]
+    return [float(v)] * G
+
+
+class BatchedSampler:
+    """Exact samples of G independent circuits in one launch per batch (see the module docstring).
+
+    circuits: [(U_g [m_g, m_g] complex CUDA tensor, in_modes_g)], shots: int or per-circuit list,
+    loss: transmission eta (scalar or per circuit), indist: x-model overlap x (scalar or per circuit),
+    precision: "f64" | "mixed", seed: seeds the device generator, graph: capture the batch in a CUDA graph,
+    tune: pick the launch shape with the autotuner (cached per GPU and workload).
+    """
+
+    def __init__(self, circuits, shots, loss=None, indist=None, precision: str = "mixed", seed: int = 0,
+                 graph: bool = True, tune: bool = True, block_threads: int = 0, tpl: int = 0):
+        if not circuits:
+            raise ValueError("at least one circuit")
+        if precision not in N.PRECISIONS:
+            raise ValueError(f"unknown precision {precision!r}: 'f64' or 'mixed'")
+        U0 = circuits[0][0]
+        N.require_cuda(U0, "U")
+        self.device = U0.device
+        dev = self.device
+        G = len(circuits)
+        for U, modes in circuits:
+            if U.dim() != 2 or U.shape[0] != U.shape[1]:
+                raise ValueError("every U must be a square [m, m] matrix")
+            if any(not 0 <= int(j) < U.shape[0] for j in modes):
+                raise ValueError("input modes must be modes of their circuit")
+        shots_l = [int(shots)] * G if not isinstance(shots, (list, tuple)) else [int(x) for x in shots]
+        if len(shots_l) != G or any(x < 0 for x in shots_l):
+            raise ValueError("shots: one non-negative count per circuit")
+        etas = _per_instance(loss, G, 1.0)
+        xs = _per_instance(indist, G, 1.0)
+        if any(not 0.0 <= e <= 1.0 for e in etas) or any(not 0.0 <= x <= 1.0 for x in xs):
+            raise ValueError("loss (transmission) and indist (x-model overlap) must lie in [0, 1]")
+        self.precision = precision
+        self.G = G
+        self.shots = shots_l
+        self.m = [int(U.shape[0]) for U, _ in circuits]
+        self.n = [len(modes) for _, modes in circuits]
+        self.m_max, self.n_stride = max(self.m), max(max(self.n), 1)
+        if self.n_stride > N.PE_MAX_PHOTONS:
+            raise ValueError(f"at most {N.PE_MAX_PHOTONS} photons per circuit")
+        self.S = sum(shots_l)
+        self.acol, self.inst_off, self.inst_m, self.inst_n = pack_ragged(circuits)
+        self.acol = torch.view_as_real(self.acol).contiguous()
+        self.dp = torch.repeat_interleave(torch.arange(G, device=dev), torch.tensor(shots_l, device=dev)).contiguous()
+        self.eta = torch.tensor(etas, dtype=torch.float64, device=dev)
+        self.x = torch.tensor(xs, dtype=torch.float64, device=dev)
+        self.singles = any(x < 1.0 for x in xs)
+        slots = 1 + self.n_stride if self.singles else 1
+        self.C = self.S * slots
+        S, C, ns = self.S, self.C, self.n_stride
+        self.key = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.seeds = torch.zeros(1, ns, dtype=torch.int64, device=dev)
+        self.cols = torch.zeros(C, ns, dtype=torch.int64, device=dev)
+        self.nk = torch.zeros(C, dtype=torch.int32, device=dev)
+        self.chain_dp = torch.zeros(C, dtype=torch.int64, device=dev)
+        self.out_row = torch.zeros(C, dtype=torch.int64, device=dev)
+        self.order = torch.arange(C, dtype=torch.int64, device=dev)
+        self.nk_sorted = torch.zeros(C, dtype=torch.int32, device=dev)
+        self.rows = torch.zeros(C, ns, dtype=torch.int64, device=dev)
+        self.occ = torch.zeros(S, self.m_max, dtype=torch.int64, device=dev)
+        self.status = torch.zeros(2, dtype=torch.int32, device=dev)
+        self.ws = N.workspace(dev)
+        self.gen = torch.Generator(device=dev).manual_seed(seed)
+        self._row0 = [0]
+        for s_ in shots_l:
+            self._row0.append(self._row0[-1] + s_)
+        self.tpl, self.block = tpl, block_threads
+        if tune and not (tpl and block_threads):
+            self._autotune()
+        self.graph = None
+        if graph:
+            self._capture()
+
+    # ---------------------------------------------------------------------------------------- one batch
+    def _draw_keys(self):
+        r = torch.randint(0, 2 ** 31 - 1, (1 + self.n_stride,), generator=self.gen, device=self.device)
+        self.key.copy_(r[:1])
+        self.seeds.copy_(r[1:].view(1, -1))
+
+    def _partition(self):
+        st = N.stream_handle(self.device)
+        L = N.load()
+        N.check(L.pe_partition_shots(N.ptr(self.dp), N.ptr(self.inst_n), N.ptr(self.eta), N.ptr(self.x), self.S,
+                                     self.n_stride, int(self.singles), N.ptr(self.key), N.ptr(self.cols), N.ptr(self.nk),
+                                     N.ptr(self.chain_dp), N.ptr(self.out_row), N.ptr(self.status[:1]), st),
+                "pe_partition_shots")
+        torch.sort(self.nk, descending=True, stable=True, out=(self.nk_sorted, self.order))   # longest chains first
+
+    def _chains(self, tpl=None, block=None):
+        st = N.stream_handle(self.device)
+        L = N.load()
+        rc = L.pe_fock_chain(N.PRECISIONS[self.precision], N.ptr(self.acol), N.ptr(self.inst_off), N.ptr(self.inst_m),
+                             N.ptr(self.inst_n), self.G, self.m_max, self.C, N.ptr(self.chain_dp), N.ptr(self.nk),
+                             N.ptr(self.cols), self.n_stride, None, N.ptr(self.seeds), None, None, N.ptr(self.order),
+                             N.ptr(self.rows), None, self.m_max, None, self.m_max, N.ptr(self.ws), self.ws.numel(),
+                             int(self.block if block is None else block), int(self.tpl if tpl is None else tpl), 0, st)
+        N.check(rc, "pe_fock_chain")
+
+    def _scatter(self):
+        N.check(N.load().pe_scatter_occupations(N.ptr(self.rows), N.ptr(self.nk), N.ptr(self.out_row), self.C,
+                                                self.n_stride, N.ptr(self.occ), self.m_max, self.S,
+                                                N.ptr(self.status[1:]), N.stream_handle(self.device)),
+                "pe_scatter_occupations")
+
+    def _step(self):
+        self._draw_keys()
+        self._partition()
+        self._chains()
+        self._scatter()
+
+    def _autotune(self):
+        workload = f"batch|G{self.G}|S{self.S}|m{self.m_max}|n{self.n_stride}|singles{int(self.singles)}"
+        self._draw_keys()
+        self._partition()
+        best = autotune.tune(lambda tpl, block: self._chains(tpl, block), self.device, self.precision,
+                             autotune.tier(self.n_stride), workload)
+        self.tpl, self.block = best
+
+    def _capture(self):
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            for _ in range(2):
+                self._step()
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        g.register_generator_state(self.gen)
+        with torch.cuda.graph(g, capture_error_mode="thread_local"):
+            self._step()
+        self.graph = g
+
+    # ---------------------------------------------------------------------------------------- public
+    def sample(self) -> torch.Tensor:
+        """Run one batch; returns the occupations [S_total, m_max] (a buffer reused by the next call)."""
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._step()
+        return self.occ
+
+    def rows_of(self, g: int) -> slice:
+        """Rows of circuit g in the occupation buffer (its modes are columns 0..m_g - 1)."""
+        return slice(self._row0[g], self._row0[g + 1])
+
+    def check(self) -> None:
+        """Raise when a device-side index error was recorded (synchronises)."""
+        st = self.status.cpu().tolist()
+        ws, _ = N.read_status(self.ws)
+        if any(st) or ws:
+            raise N.NativeError(f"device-side error in the batched sampler (partition {st[0]}, scatter {st[1]}, "
+                                f"chains {ws})")
