@@ -310,6 +310,123 @@ def cpu_baseline(S: int) -> dict:
             "sample": f"{S} chains of the n=20 m=400 workload, oracle/ C port, {threads} threads, {dt:.1f} s"}
 
 
+# ----------------------------------------------------------------------------------------- other configs
+def _haar_dev(m: int, seed: int, dev):
+    import torch
+    g = torch.Generator().manual_seed(seed)
+    z = torch.randn(m, m, generator=g, dtype=torch.float64) + 1j * torch.randn(m, m, generator=g, dtype=torch.float64)
+    q, r = torch.linalg.qr(z)
+    d = torch.diagonal(r)
+    return (q * (d / d.abs()).unsqueeze(0)).to(dev)
+
+
+def _config_circuits(name: str, dev):
+    """(circuits, shots, loss, indist, description) of the configurations beside the headline one."""
+    import numpy as np
+    if name == "c1":
+        return [(_haar_dev(12, 1001, dev), list(range(6)))], 10000, None, None, \
+            "n=6 m=12, 10000 shots, lossless, Haar U"
+    if name == "c3":
+        return [(_haar_dev(900, 3001, dev), list(range(30)))], 100000, 0.5, None, \
+            "n_in=30 m=900, eta=0.5 (detected k ~ Bin(30, 0.5)), 100000 shots, Haar U"
+    if name == "c4":
+        return [(_haar_dev(784, 4001, dev), list(range(28)))], 200, None, 0.95, \
+            "n=28 m=784, 200 shots, lossless, x-model indist 0.95, Haar U"
+    if name == "c5":
+        rng = np.random.default_rng(5000)
+        circuits, etas = [], []
+        for i in range(256):
+            m = int(rng.choice([16, 24, 32, 48, 64]))
+            n = int(rng.integers(4, min(12, m // 4) + 1))
+            circuits.append((_haar_dev(m, 5000 + i, dev), list(range(n))))
+            etas.append(float(rng.uniform(0.6, 1.0)))
+        return circuits, 1000, etas, None, \
+            "256 Haar circuits, m in {16,24,32,48,64}, n in 4..min(12,m/4), eta ~ U[0.6,1], 1000 shots each"
+    raise ValueError(name)
+
+
+def run_config(args):
+    """One JSON line for a configuration run through the batched sampler (one persistent launch per batch,
+    CUDA-graph replay): mixed and FP64 samples/s, roofline of the chain kernel, picks agreement, and the
+    marginal error of the mixed form on chains of the configuration."""
+    import numpy as np
+    import torch
+
+    from photonic_engines_b200 import _native as NAT
+    from photonic_engines_b200.clifford import BatchedSampler, sample_chains
+    from photonic_engines_b200.clifford.work import chain_work
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    circuits, shots, loss, indist, desc = _config_circuits(args.config, dev)
+    peak = {"f64": NAT.pipe_peak_tflops("f64", dev), "mixed": NAT.pipe_peak_tflops("mixed", dev)}
+    out = {}
+    occs = {}
+    for precision in ("mixed", "f64"):
+        bs = BatchedSampler(circuits, shots, loss=loss, indist=indist, precision=precision, seed=7, tune=True)
+        for _ in range(args.warmup):
+            bs.sample()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        work = []
+        with ClockSampler(0) as clk:
+            e0.record()
+            for _ in range(args.steps):
+                bs.sample()
+            e1.record()
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        bs.check()
+        nk = bs.nk.cpu().numpy()
+        rows = bs.rows.cpu().numpy()
+        flops = 0.0
+        for g in range(bs.G):                                # work of the last batch, per circuit (m differs)
+            sel = (bs.chain_dp.cpu().numpy() == g) & (nk > 0)
+            if sel.any():
+                flops += chain_work(rows[sel], bs.m[g], nk[sel])["flops"]
+        occs[precision] = bs.occ.clone()
+        bound = "fp32" if precision == "mixed" else "fp64"
+        ach = flops / (ms * 1e-3) / 1e12
+        out[precision] = {"value": bs.S / (ms * 1e-3), "ms_per_step": ms, "tpl_block": [bs.tpl, bs.block],
+                          "roofline": {"bound": bound, "achieved": ach, "peak": peak[precision], "unit": "TFLOP/s",
+                                       "frac": ach / peak[precision], "traffic": None,
+                                       "peak_source": "measured live by pe_pipe_probe", "flops_per_launch": flops},
+                          "clocks": clk.summary()}
+        # end to end: the same batch with the occupations copied to pinned host memory every step
+        host = torch.empty_like(bs.occ, device="cpu").pin_memory()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.steps):
+            host.copy_(bs.sample(), non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        out[precision]["e2e"] = {"value": bs.S / (e0.elapsed_time(e1) * 1e-3 / args.steps), "unit": "samples/s",
+                                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": bs.occ.numel() * 8}
+        del bs
+    # marginal error of the mixed form against the FP64 form on lossless chains of each circuit
+    rng = np.random.default_rng(3)
+    max_err, per_k = 0.0, {}
+    inst = circuits if len(circuits) <= 8 else [circuits[i] for i in range(0, len(circuits), len(circuits) // 16)]
+    for U, modes in inst:
+        n = len(modes)
+        S = 8 if n >= 26 else 32
+        sig = np.argsort(rng.random((S, n)), axis=1)
+        u = rng.random((S, n))
+        a = sample_chains(U, modes, sig, uniforms=u, want_marg=True)
+        b = sample_chains(U, modes, sig, uniforms=u, want_marg=True, precision="mixed")
+        err = ((b["marg"] - a["marg"]).abs().amax(2) / a["marg"].abs().amax(2)).cpu().numpy()
+        max_err = max(max_err, float(err.max()))
+        for k in range(n):
+            per_k[k + 1] = max(per_k.get(k + 1, 0.0), float(err[:, k].max()))
+    line = {"config": args.config, "workload": desc, "metric": "samples/s", "unit": "samples/s",
+            "value": out["mixed"]["value"], "fp64": out["f64"], "mixed": out["mixed"],
+            "mixed_over_fp64": out["mixed"]["value"] / out["f64"]["value"],
+            "occupations_equal_fp64": bool(torch.equal(occs["mixed"], occs["f64"])),
+            "max_marginal_rel_err": max_err, "marginal_err_by_k": per_k, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
 def profile_launch(precision: str):
     """One warm-up launch and one launch of the chain kernel on the benchmark workload (for ncu -s 1 -c 1)."""
     import torch
@@ -340,6 +457,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--ref-shots", type=int, default=0, help="chains per CPU sample (0: scaled to the cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", choices=("c1", "c2", "c3", "c4", "c5"), default="c2",
+                    help="c2 (default) is the headline line; the others print one line through the batched sampler")
     ap.add_argument("--profile-launch", choices=("f64", "mixed"), default=None,
                     help="run only two chain launches of the workload (a target for ncu -s 1 -c 1)")
     args = ap.parse_args()
@@ -348,6 +467,9 @@ def main():
         return
     if args.warmup < 3:
         args.warmup = 3
+    if args.config != "c2" and args.impl == "b200":
+        run_config(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
