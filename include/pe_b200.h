@@ -84,6 +84,27 @@ int pe_fock_chain(int precision, const double* d_acol, const int64_t* d_inst_off
                   int grid_ctas, void* stream);
 
 /*
+ * The same chains with the heavy steps spread over several CTAs per stream, for batches with few
+ * streams (down to one sample) where one CTA per stream leaves most SMs idle.  Steps 1..k_split-1 run
+ * in the persistent kernel; every step k >= k_split runs as nch CTAs per stream, each summing its share
+ * of the Gray lanes into a partial (workspace), then one CTA per stream sums the partials in a fixed
+ * order and draws.  Same results as pe_fock_chain up to the rounding of the partial sums (FP64:
+ * within 1e-12).  Workspace: pe_chain_split_workspace_bytes(S, nch).  k_split >= 2, nch >= 1.
+ * Replaces, beside the step loop: photonic_engines/clifford/single.py:22-82 (fock_sample_single: one
+ * sample over a fixed lane grid) and the lane planning of cofactors_triton.py:450-465.
+ */
+int pe_fock_chain_split(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
+                        const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
+                        const int32_t* d_nk, const int64_t* d_cols, int n_stride, const double* d_uniforms,
+                        const int64_t* d_seeds, const int64_t* d_seed_row, const int64_t* d_rng_off,
+                        const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
+                        int marg_stride, int k_split, int nch, void* d_workspace, size_t workspace_bytes,
+                        int block_threads, int tpl, void* stream);
+
+/* Bytes of device workspace pe_fock_chain_split needs for S streams and nch CTAs per stream. */
+size_t pe_chain_split_workspace_bytes(int64_t S, int nch);
+
+/*
  * pe_fock_chain without a workspace argument: the same chains and outputs, for callers that cannot
  * allocate device memory when they sample (a host callback or other context where CUDA allocation is not
  * allowed, a serving process whose device memory all belongs to its own arena, a foreign-language

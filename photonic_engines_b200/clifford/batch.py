@@ -19,7 +19,7 @@ import torch
 
 from .. import _native as N
 from .. import autotune
-from .kernels import pack_ragged
+from .kernels import pack_ragged, split_plan
 
 
 def _per_instance(v, G, default):
@@ -93,7 +93,12 @@ class BatchedSampler:
         self.rows = torch.zeros(C, ns, dtype=torch.int64, device=dev)
         self.occ = torch.zeros(S, self.m_max, dtype=torch.int64, device=dev)
         self.status = torch.zeros(2, dtype=torch.int32, device=dev)
-        self.ws = N.workspace(dev)
+        self.split = split_plan(self.S, self.n_stride, dev, 256, 2)      # few long chains: share their steps
+        if self.split:
+            self.ws = torch.empty(int(N.load().pe_chain_split_workspace_bytes(C, self.split[1])), dtype=torch.uint8,
+                                  device=dev)
+        else:
+            self.ws = N.workspace(dev)
         self.gen = torch.Generator(device=dev).manual_seed(seed)
         self._row0 = [0]
         for s_ in shots_l:
@@ -123,11 +128,17 @@ class BatchedSampler:
     def _chains(self, tpl=None, block=None):
         st = N.stream_handle(self.device)
         L = N.load()
-        rc = L.pe_fock_chain(N.PRECISIONS[self.precision], N.ptr(self.acol), N.ptr(self.inst_off), N.ptr(self.inst_m),
-                             N.ptr(self.inst_n), self.G, self.m_max, self.C, N.ptr(self.chain_dp), N.ptr(self.nk),
-                             N.ptr(self.cols), self.n_stride, None, N.ptr(self.seeds), None, None, N.ptr(self.order),
-                             N.ptr(self.rows), None, self.m_max, None, self.m_max, N.ptr(self.ws), self.ws.numel(),
-                             int(self.block if block is None else block), int(self.tpl if tpl is None else tpl), 0, st)
+        common = (N.PRECISIONS[self.precision], N.ptr(self.acol), N.ptr(self.inst_off), N.ptr(self.inst_m),
+                  N.ptr(self.inst_n), self.G, self.m_max, self.C, N.ptr(self.chain_dp), N.ptr(self.nk), N.ptr(self.cols),
+                  self.n_stride, None, N.ptr(self.seeds), None, None, N.ptr(self.order), N.ptr(self.rows), None,
+                  self.m_max, None, self.m_max)
+        block = int(self.block if block is None else block)
+        tpl = int(self.tpl if tpl is None else tpl)
+        if self.split:
+            rc = L.pe_fock_chain_split(*common, self.split[0], self.split[1], N.ptr(self.ws), self.ws.numel(), block,
+                                       tpl, st)
+        else:
+            rc = L.pe_fock_chain(*common, N.ptr(self.ws), self.ws.numel(), block, tpl, 0, st)
         N.check(rc, "pe_fock_chain")
 
     def _scatter(self):

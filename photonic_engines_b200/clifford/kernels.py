@@ -56,14 +56,32 @@ def _i64(t, dev):
     return None if t is None else torch.as_tensor(t, dtype=torch.int64, device=dev).contiguous()
 
 
+def split_plan(heavy_streams: int, n: int, device, block_threads: int = 256, tpl: int = 2):
+    """(k_split, nch) for a batch whose long chains number `heavy_streams`, or None when one CTA per stream
+    already fills the GPU.  nch CTAs share every step k >= k_split of a stream; k_split is the first step
+    with enough Gray terms (2^(k-2)) for every CTA to run several lanes."""
+    slots = 2 * torch.cuda.get_device_properties(device).multi_processor_count
+    if heavy_streams >= slots or n < 8:
+        return None
+    nch = min(64, -(-2 * slots // max(heavy_streams, 1)))
+    lanes = (block_threads or 256) // max(tpl, 1)
+    k = 2
+    while k <= n and (1 << (k - 2)) < 4 * nch * lanes:
+        k += 1
+    return (k, nch) if k <= n else None
+
+
 def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst_n: torch.Tensor, dp, cols, *,
           m_max: int | None = None, nk=None, uniforms=None, seeds=None, seed_row=None, rng_off=None, order=None,
           want_occ: bool = True, occ_stride: int | None = None, want_marg: bool = False, precision: str = "f64",
-          block_threads: int = 0, tpl: int = 0, grid_ctas: int = 0, check_status: bool = True, out=None):
+          block_threads: int = 0, tpl: int = 0, grid_ctas: int = 0, check_status: bool = True, out=None,
+          split=None):
     """Run the chains of S streams.  dp [S] instance per stream, cols [S, n_stride] input columns in chain order,
     nk [S] photons per stream (None: n_stride), uniforms [S, n_stride] (None: Philox from seeds [R, n_stride],
     seed_row [S], rng_off [S]).  Returns (rows [S, n_stride] int64, occ [S, occ_stride] or None,
-    marg [S, n_stride, m_max] or None).  `out` may hold preallocated (rows, occ, marg) tensors."""
+    marg [S, n_stride, m_max] or None).  `out` may hold preallocated (rows, occ, marg) tensors.
+    split: (k_split, nch) spreads every step k >= k_split over nch CTAs per stream (few-stream batches);
+    None or False runs each stream in one CTA."""
     N.require_cuda(acol, "acol")
     dev = acol.device
     L = N.load()
@@ -92,15 +110,22 @@ def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst
         rows = torch.zeros(S, n_stride, dtype=torch.int64, device=dev)
         occ = torch.empty(S, occ_stride, dtype=torch.int64, device=dev) if want_occ else None
         marg = torch.zeros(S, n_stride, m_max, dtype=torch.float64, device=dev) if want_marg else None
-    ws = N.workspace(dev)
     a = acol if acol.dtype == torch.float64 else torch.view_as_real(acol.contiguous())
-    rc = L.pe_fock_chain(N.PRECISIONS[precision], N.ptr(a), N.ptr(inst_off), N.ptr(inst_m), N.ptr(inst_n),
-                         int(inst_off.shape[0]), int(m_max), int(S), N.ptr(dp), N.ptr(nk_t), N.ptr(cols), int(n_stride),
-                         N.ptr(u_t), N.ptr(seeds_t), N.ptr(_i64(seed_row, dev)), N.ptr(_i64(rng_off, dev)),
-                         N.ptr(_i64(order, dev)), N.ptr(rows), N.ptr(occ), int(occ_stride), N.ptr(marg),
-                         int(m_max), N.ptr(ws), int(ws.numel()), int(block_threads), int(tpl), int(grid_ctas),
-                         N.stream_handle(dev))
-    N.check(rc, "pe_fock_chain")
+    common = (N.PRECISIONS[precision], N.ptr(a), N.ptr(inst_off), N.ptr(inst_m), N.ptr(inst_n), int(inst_off.shape[0]),
+              int(m_max), int(S), N.ptr(dp), N.ptr(nk_t), N.ptr(cols), int(n_stride), N.ptr(u_t), N.ptr(seeds_t),
+              N.ptr(_i64(seed_row, dev)), N.ptr(_i64(rng_off, dev)), N.ptr(_i64(order, dev)), N.ptr(rows), N.ptr(occ),
+              int(occ_stride), N.ptr(marg), int(m_max))
+    if split:
+        k_split, nch = split
+        ws = torch.empty(int(L.pe_chain_split_workspace_bytes(S, nch)), dtype=torch.uint8, device=dev)
+        rc = L.pe_fock_chain_split(*common, int(k_split), int(nch), N.ptr(ws), int(ws.numel()), int(block_threads),
+                                   int(tpl), N.stream_handle(dev))
+        N.check(rc, "pe_fock_chain_split")
+    else:
+        ws = N.workspace(dev)
+        rc = L.pe_fock_chain(*common, N.ptr(ws), int(ws.numel()), int(block_threads), int(tpl), int(grid_ctas),
+                             N.stream_handle(dev))
+        N.check(rc, "pe_fock_chain")
     if check_status:
         st, det = N.read_status(ws)
         if st != 0:

@@ -23,7 +23,7 @@ import torch
 
 from .. import _native as N
 from ..imperfections import partition, route_classical, spec
-from .kernels import chain, pack_instances
+from .kernels import chain, pack_instances, split_plan
 
 BACKENDS = ("b200", "triton", "cuda", "exq")
 ALGOS = ("auto", "2018", "2020", "input", "percof")
@@ -61,10 +61,12 @@ def _pass_draws(S: int, k: int, generator, dev, max_streams: int):
 
 def sample_chains(U, in_modes, sigma, *, uniforms=None, seeds=None, seed_row=None, rng_off=None, dp=None,
                   precision: str = "f64", want_marg: bool = False, block_threads: int = 0, tpl: int = 0,
-                  grid_ctas: int = 0):
+                  grid_ctas: int = 0, split=False):
     """The chains of S streams with a GIVEN column order: sigma [S, n] (indices into in_modes), per-step
     uniforms [S, n] (or the reference's Philox draws from seeds [n] / [R, n]).  dp [S]: circuit of each stream
     (default: all circuit 0 when U is [m, m], else b * shots layout is the caller's).
+    split: False (one CTA per stream), None (spread heavy steps over several CTAs when the streams are too
+    few to fill the GPU) or an explicit (k_split, nch).
     Returns dict(rows [S, n] ordered output modes, occ [S, m], marg [S, n, m] or None)."""
     N.require_cuda(U, "U")
     if U.dim() == 2:
@@ -75,9 +77,12 @@ def sample_chains(U, in_modes, sigma, *, uniforms=None, seeds=None, seed_row=Non
     if dp is None:
         dp = torch.zeros(S, dtype=torch.int64, device=dev)
     acol, inst_off, inst_m, inst_n = pack_instances(U, in_modes)
+    if split is None:
+        split = split_plan(S, n, dev, block_threads or 256, tpl or 2)
     rows, occ, marg = chain(acol, inst_off, inst_m, inst_n, dp, sigma, uniforms=uniforms, seeds=seeds,
                             seed_row=seed_row, rng_off=rng_off, want_occ=True, want_marg=want_marg,
-                            precision=precision, block_threads=block_threads, tpl=tpl, grid_ctas=grid_ctas)
+                            precision=precision, block_threads=block_threads, tpl=tpl, grid_ctas=grid_ctas,
+                            split=split)
     return {"rows": rows, "occ": occ, "marg": marg}
 
 
@@ -152,9 +157,11 @@ def fock_sample(U, in_modes, shots, generator=None, algo="auto", multi_min_k1=10
     direct = plan.out_row is None
     if plan.C > 0:
         u = None if uniforms is None else torch.as_tensor(uniforms, dtype=torch.float64, device=dev)
+        heavy = plan.C if plan.nk is None else int((plan.nk >= 8).sum())
         rows, occ_k, _ = chain(acol, inst_off, inst_m, inst_n, plan.dp, plan.cols, m_max=m, nk=plan.nk, uniforms=u,
                                seeds=plan.seeds, seed_row=plan.seed_row, rng_off=plan.rng_off, order=plan.order,
-                               want_occ=direct, precision=precision, block_threads=block_threads, tpl=tpl)
+                               want_occ=direct, precision=precision, block_threads=block_threads, tpl=tpl,
+                               split=split_plan(heavy, n, dev, block_threads or 256, tpl or 2))
         if direct:
             occ = occ_k
     if stats is not None:

@@ -24,12 +24,25 @@ static int kpm_index(int kpm) {
 
 static void* g_chain[2][3][N_KPM];
 static void* g_cof[2][3][N_KPM];
+static void* g_split_partial[2][3][N_KPM];
+static void* g_split_draw[2][N_KPM];
 
-void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cofactor_kernel) {
+void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cofactor_kernel, void* split_partial,
+                      void* split_draw) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
     if (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) return;
     g_chain[mixed][ti][ki] = chain_kernel;
     g_cof[mixed][ti][ki] = cofactor_kernel;
+    g_split_partial[mixed][ti][ki] = split_partial;
+    g_split_draw[mixed][ki] = split_draw;
+}
+void* find_split_partial_kernel(int mixed, int tpl, int kpm) {
+    const int ti = tpl_index(tpl), ki = kpm_index(kpm);
+    return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_split_partial[mixed][ti][ki];
+}
+void* find_split_draw_kernel(int mixed, int kpm) {
+    const int ki = kpm_index(kpm);
+    return (mixed < 0 || mixed > 1 || ki < 0) ? nullptr : g_split_draw[mixed][ki];
 }
 void* find_chain_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
@@ -117,20 +130,27 @@ static int launch_prepare(void* fn, int block, size_t smem, int* grid_per_sm) {
     return PE_OK;
 }
 
-extern "C" int pe_fock_chain(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
-                             const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
-                             const int32_t* d_nk, const int64_t* d_cols, int n_stride, const double* d_uniforms,
-                             const int64_t* d_seeds, const int64_t* d_seed_row, const int64_t* d_rng_off,
-                             const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
-                             int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
-                             int grid_ctas, void* stream) {
+// Checks, variant lookup and launches shared by the chain entry points.  k_split = 0: the whole chain in
+// the persistent kernel; k_split >= 2: steps 1..k_split-1 there, then every step k >= k_split spread over
+// nch CTAs per stream (split_partial) and drawn by one CTA per stream (split_draw).
+static int chain_launch(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
+                        const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
+                        const int32_t* d_nk, const int64_t* d_cols, int n_stride, const double* d_uniforms,
+                        const int64_t* d_seeds, const int64_t* d_seed_row, const int64_t* d_rng_off,
+                        const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
+                        int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
+                        int grid_ctas, int k_split, int nch, void* stream) {
     if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
     if (S < 0 || G < 1 || m_max < 1 || n_stride < 1) return PE_ERR_ARG;
     if (!d_acol || !d_inst_off || !d_inst_m || !d_inst_n || !d_dp || !d_cols || !d_rows || !d_workspace) return PE_ERR_ARG;
     if (!d_uniforms && !d_seeds) return PE_ERR_ARG;
     if (d_occ && occ_stride < m_max) return PE_ERR_ARG;
     if (d_marg && marg_stride < m_max) return PE_ERR_ARG;
-    if (workspace_bytes < WS_BYTES || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
+    if (k_split < 0 || (k_split > 0 && (k_split < 2 || nch < 1))) return PE_ERR_ARG;
+    const bool split = k_split > 0 && k_split <= n_stride;
+    const size_t part_bytes = split ? (size_t)S * nch * MAXN * sizeof(double2) : 0;
+    const size_t need = WS_BYTES + part_bytes + (split ? (size_t)S * sizeof(int) : 0);
+    if (workspace_bytes < need || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
     const int kpm = kpm_for(n_stride);
     if (kpm < 0) return PE_ERR_SIZE;
     if (tpl == 0) tpl = default_tpl(kpm);
@@ -138,7 +158,7 @@ extern "C" int pe_fock_chain(int precision, const double* d_acol, const int64_t*
     void* fn = find_chain_kernel(precision, tpl, kpm);
     if (!fn) return PE_ERR_SIZE;
     const int block = block_threads ? block_threads : 256;
-    if (block < 32 || block > 256 || (block & 31) || block < 32 * 1) return PE_ERR_ARG;
+    if (block < 32 || block > 256 || (block & 31)) return PE_ERR_ARG;
     const size_t smem = smem_fixed_bytes() + (size_t)m_max * sizeof(double);
     const int cap = max_smem_optin();
     if (cap <= 0) return PE_ERR_CUDA;
@@ -165,10 +185,73 @@ extern "C" int pe_fock_chain(int precision, const double* d_acol, const int64_t*
     p.status = (int*)((char*)d_workspace + 8);
     p.detail = (long long*)((char*)d_workspace + 16);
     p.m_cap = m_max;
-    p.tau = 3.0e-5;
+    p.tau = 1.0e-5;            // mixed guard band: 3x the largest measured CDF deviation (3.3e-6, n <= 28)
+    p.k_stop = split ? k_split - 1 : 0;
     void* args[] = {&p};
     if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st) != cudaSuccess) return PE_ERR_CUDA;
+    if (!split) return PE_OK;
+    // the mixed form's guard band: flagged streams redo the step with the FP64 kernels (second pass)
+    const int npass = precision == PE_PRECISION_MIXED ? 2 : 1;
+    void* fpart[2] = {find_split_partial_kernel(precision, tpl, kpm), find_split_partial_kernel(PE_PRECISION_F64, tpl, kpm)};
+    void* fdraw[2] = {find_split_draw_kernel(precision, kpm), find_split_draw_kernel(PE_PRECISION_F64, kpm)};
+    int64_t gpart[2], gdraw[2];
+    const int64_t items = S * (int64_t)nch;
+    for (int q = 0; q < npass; ++q) {
+        if (!fpart[q] || !fdraw[q]) return PE_ERR_SIZE;
+        int per_part = 0, per_draw = 0;
+        if ((rc = launch_prepare(fpart[q], block, smem_fixed_bytes(), &per_part)) != PE_OK) return rc;
+        if ((rc = launch_prepare(fdraw[q], block, smem, &per_draw)) != PE_OK) return rc;
+        gpart[q] = items < (int64_t)sms * per_part ? items : (int64_t)sms * per_part;
+        gdraw[q] = S < (int64_t)sms * per_draw ? S : (int64_t)sms * per_draw;
+    }
+    SplitParams sp;
+    sp.c = p;
+    sp.nch = nch;
+    sp.partial = (double2*)((char*)d_workspace + WS_BYTES);
+    sp.flag = (int*)((char*)d_workspace + WS_BYTES + part_bytes);
+    void* sargs[] = {&sp};
+    for (int k = k_split; k <= n_stride; ++k) {
+        sp.k = k;
+        for (int q = 0; q < npass; ++q) {
+            sp.pass = q;
+            if (cudaLaunchKernel(fpart[q], dim3((unsigned)gpart[q]), dim3(block), sargs, smem_fixed_bytes(), st) !=
+                cudaSuccess)
+                return PE_ERR_CUDA;
+            if (cudaLaunchKernel(fdraw[q], dim3((unsigned)gdraw[q]), dim3(block), sargs, smem, st) != cudaSuccess)
+                return PE_ERR_CUDA;
+        }
+    }
     return PE_OK;
+}
+
+extern "C" int pe_fock_chain(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
+                             const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
+                             const int32_t* d_nk, const int64_t* d_cols, int n_stride, const double* d_uniforms,
+                             const int64_t* d_seeds, const int64_t* d_seed_row, const int64_t* d_rng_off,
+                             const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
+                             int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
+                             int grid_ctas, void* stream) {
+    return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, d_nk, d_cols, n_stride,
+                        d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ, occ_stride, d_marg,
+                        marg_stride, d_workspace, workspace_bytes, block_threads, tpl, grid_ctas, 0, 1, stream);
+}
+
+extern "C" size_t pe_chain_split_workspace_bytes(int64_t S, int nch) {
+    const size_t s = (size_t)(S < 0 ? 0 : S);
+    return WS_BYTES + s * (size_t)(nch < 1 ? 1 : nch) * MAXN * sizeof(double2) + s * sizeof(int);
+}
+
+extern "C" int pe_fock_chain_split(int precision, const double* d_acol, const int64_t* d_inst_off,
+                                   const int32_t* d_inst_m, const int32_t* d_inst_n, int G, int m_max, int64_t S,
+                                   const int64_t* d_dp, const int32_t* d_nk, const int64_t* d_cols, int n_stride,
+                                   const double* d_uniforms, const int64_t* d_seeds, const int64_t* d_seed_row,
+                                   const int64_t* d_rng_off, const int64_t* d_order, int64_t* d_rows, int64_t* d_occ,
+                                   int occ_stride, double* d_marg, int marg_stride, int k_split, int nch,
+                                   void* d_workspace, size_t workspace_bytes, int block_threads, int tpl, void* stream) {
+    if (k_split < 2 || nch < 1) return PE_ERR_ARG;
+    return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, d_nk, d_cols, n_stride,
+                        d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ, occ_stride, d_marg,
+                        marg_stride, d_workspace, workspace_bytes, block_threads, tpl, 0, k_split, nch, stream);
 }
 
 extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t* d_rows, int64_t S, int m, int K,

@@ -13,7 +13,9 @@ struct Registration {
     Registration() {
         pe::register_variant(PE_MIXED, PE_TPL, PE_KPM,
                              (void*)pe::fock_chain_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
-                             (void*)pe::cofactor_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>);
+                             (void*)pe::cofactor_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
+                             (void*)pe::split_partial_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
+                             (void*)pe::split_draw_kernel<PE_KPM, (PE_MIXED != 0)>);
     }
 };
 Registration registration;

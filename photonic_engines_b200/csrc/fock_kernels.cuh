@@ -68,6 +68,7 @@ struct ChainParams {
     long long* detail;
     int m_cap;
     double tau;     // mixed form: relative guard band of the draw
+    int k_stop;     // run steps 1..min(nk, k_stop) only (0: all); later steps go to the split kernels
 };
 
 // Mixed form: FP32 inner blocks of at most this many terms, each starting from FP64 column sums.
@@ -611,7 +612,7 @@ __device__ void sweep_f64(Smem& sm) {
     double ar[KH], ai[KH];
 #pragma unroll
     for (int j = 0; j < KH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
-    for (int64_t hl = lane; hl < H; hl += lanes) {
+    for (int64_t hl = sm.lane0 + lane; hl < H; hl += (int64_t)lanes * sm.lane_mult) {
         double sr[KH], si[KH], wh;
         const uint64_t hpack = lane_digits(pl, hl, &wh);
         lane_sums<KH>(sm, c0, false, 0, hl, hpack, sr, si);
@@ -647,7 +648,7 @@ __device__ void sweep_mixed(Smem& sm) {
     double ar[KH], ai[KH];
 #pragma unroll
     for (int j = 0; j < KH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
-    for (int64_t hl = lane; hl < H; hl += lanes) {
+    for (int64_t hl = sm.lane0 + lane; hl < H; hl += (int64_t)lanes * sm.lane_mult) {
         double wh;
         const uint64_t hpack = lane_digits(pl, hl, &wh);
         for (int pm = 0; pm < Lmid; ++pm) {
@@ -708,7 +709,7 @@ __device__ void dispatch_mixed(Smem& sm, int K) {
 // One cofactor step of the stream held in shared memory (K1 >= 1): plan, prepare, sweep.
 template <int TPL, int KPM, bool MIXED>
 __device__ __forceinline__ void cofactor_step(Smem& sm, const double2* A, int64_t rs, int64_t cs, int K1, int K) {
-    if (threadIdx.x < 32) plan_step(sm, K1, K, blockDim.x / TPL, MIXED ? MIXED_LIN : LIN_MAX);
+    if (threadIdx.x < 32) plan_step(sm, K1, K, blockDim.x / TPL * sm.lane_mult, MIXED ? MIXED_LIN : LIN_MAX);
     __syncthreads();
     prepare_step(sm, A, rs, cs, MIXED);
     __syncthreads();
@@ -809,14 +810,15 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
         else sm.cols[tid] = (int)c;
     }
     if (!ok && tid == 0) sm.bad = 1;
-    if (tid == 0) sm.ngrp = 0;
+    if (tid == 0) { sm.ngrp = 0; sm.lane0 = 0; sm.lane_mult = 1; }
     __syncthreads();
     if (sm.bad) {
         if (tid == 0) record_error(p.status, p.detail, s);
         return;
     }
     const double2* A = p.acol + off;      // (rho, j) at A[j * m + rho]
-    for (int k = 1; k <= nk; ++k) {
+    const int kend = (p.k_stop > 0 && p.k_stop < nk) ? p.k_stop : nk;
+    for (int k = 1; k <= kend; ++k) {
         const int K = k, K1 = k - 1;
         if (K1 == 0) {
             if (tid == 0) sm.P[0] = make_double2(1.0, 0.0);
@@ -845,8 +847,8 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
             draw_step(sm, wgt, A, 1, m, m, k, u, mrow, true);
         }
     }
-    for (int j = tid; j < nk; j += blockDim.x) p.rows[s * p.n_stride + j] = sm.rows[j];
-    if (p.occ) {
+    for (int j = tid; j < kend; j += blockDim.x) p.rows[s * p.n_stride + j] = sm.rows[j];
+    if (p.occ && kend == nk) {
         for (int rho = tid; rho < p.occ_stride; rho += blockDim.x) {
             int c = 0;
             for (int j = 0; j < nk; ++j) c += (sm.rows[j] == rho) ? 1 : 0;
@@ -881,6 +883,130 @@ __global__ void __launch_bounds__(256, PE_MINB) fock_chain_kernel(ChainParams p)
     }
 }
 
+// ---------------------------------------------------------------------------------------- split steps
+// A heavy step of few streams spread over several CTAs per stream: `split_partial_kernel` computes, for
+// work item (stream s, chunk i), the Gray lanes i*lanes + j*(nch*lanes) of step k into
+// partial[s][i][:]; `split_draw_kernel` sums a stream's chunks in a fixed order and draws.  The stream
+// state between steps (rows chosen so far) lives in the rows output.
+struct SplitParams {
+    ChainParams c;
+    int k;                  // the step (k columns, k - 1 chosen rows), k >= 2
+    int nch;                // CTAs per stream at this step
+    double2* partial;       // [S][nch][MAXN]
+    int* flag;              // [S] mixed form: 1 when the draw fell in the guard band (redo this step in FP64)
+    int pass;               // 0: the step; 1: only the flagged streams (FP64 kernels)
+};
+
+// Stream state of step k from global memory into shared memory; false when the stream has fewer photons
+// than k (nothing to do) or an index is out of range (recorded).  Uniform across the CTA.
+static __device__ bool load_state(const ChainParams& p, Smem& sm, int64_t s, int k, int& m, int64_t& off) {
+    const int tid = threadIdx.x;
+    if (tid == 0) { sm.bad = 0; sm.ngrp = 0; }
+    __syncthreads();
+    const int64_t g = p.dp[s];
+    bool ok = g >= 0 && g < p.G;
+    int nin = 0;
+    m = 0;
+    off = 0;
+    if (ok) { m = p.inst_m[g]; nin = p.inst_n[g]; off = p.inst_off[g]; }
+    const int nk = p.nk ? p.nk[s] : p.n_stride;
+    if (ok && nk < k) return false;
+    ok = ok && nk <= p.n_stride && m >= 1 && m <= p.m_cap && m <= p.occ_stride;
+    if (ok && tid < k) {
+        const int64_t c = p.cols[s * p.n_stride + tid];
+        if (c < 0 || c >= nin) atomicOr(&sm.bad, 1);
+        else sm.cols[tid] = (int)c;
+    }
+    if (ok && tid < k - 1) {
+        const int64_t r = p.rows[s * p.n_stride + tid];
+        if (r < 0 || r >= m) atomicOr(&sm.bad, 1);
+        else sm.rows[tid] = (int)r;
+    }
+    if (!ok && tid == 0) sm.bad = 1;
+    __syncthreads();
+    if (sm.bad) {
+        if (tid == 0) record_error(p.status, p.detail, s);
+        return false;
+    }
+    if (tid == 0) for (int i = 0; i < k - 1; ++i) add_to_groups(sm, sm.rows[i]);
+    __syncthreads();
+    return true;
+}
+
+template <int TPL, int KPM, bool MIXED>
+__global__ void __launch_bounds__(256, PE_MINB) split_partial_kernel(SplitParams sp) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+    const ChainParams& p = sp.c;
+    const int tid = threadIdx.x, k = sp.k;
+    for (int64_t item = blockIdx.x; item < p.S * sp.nch; item += gridDim.x) {
+        const int64_t s = item / sp.nch;
+        const int i = (int)(item % sp.nch);
+        int m;
+        int64_t off;
+        const bool live = load_state(p, sm, s, k, m, off) && (sp.pass == 0 || sp.flag[s] != 0);
+        if (live) {
+            if (tid == 0) { sm.lane0 = (int64_t)i * (blockDim.x / TPL); sm.lane_mult = sp.nch; }
+            __syncthreads();
+            cofactor_step<TPL, KPM, MIXED>(sm, p.acol + off, 1, m, k - 1, k);
+            if (tid < k) sp.partial[(s * sp.nch + i) * MAXN + tid] = sm.P[tid];
+        }
+        __syncthreads();
+    }
+}
+
+template <int KPM, bool MIXED>
+__global__ void __launch_bounds__(256, PE_MINB) split_draw_kernel(SplitParams sp) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+    double* wgt = reinterpret_cast<double*>(smem_raw + ((sizeof(Smem) + 15) & ~(size_t)15));
+    const ChainParams& p = sp.c;
+    const int tid = threadIdx.x, k = sp.k;
+    for (int64_t s = blockIdx.x; s < p.S; s += gridDim.x) {
+        int m;
+        int64_t off;
+        if (!load_state(p, sm, s, k, m, off) || (sp.pass == 1 && sp.flag[s] == 0)) { __syncthreads(); continue; }
+        if (tid < k) {
+            double xr = 0.0, xi = 0.0;
+            for (int i = 0; i < sp.nch; ++i) {
+                const double2 v = sp.partial[(s * sp.nch + i) * MAXN + tid];
+                xr += v.x;
+                xi += v.y;
+            }
+            sm.P[tid] = make_double2(xr, xi);
+        }
+        __syncthreads();
+        const double2* A = p.acol + off;
+        double u;
+        if (p.uniforms) {
+            u = p.uniforms[s * p.n_stride + (k - 1)];
+        } else {
+            const int64_t row = p.seed_row ? p.seed_row[s] : 0;
+            const int64_t ro = p.rng_off ? p.rng_off[s] : s;
+            u = chain_uniform((uint64_t)p.seeds[row * p.n_stride + (k - 1)], ro);
+        }
+        double* mrow = p.marg ? p.marg + ((size_t)s * p.n_stride + (k - 1)) * p.marg_stride : nullptr;
+        draw_step(sm, wgt, A, 1, m, m, k, u, mrow, false);
+        if constexpr (MIXED) {
+            const bool redo = sm.fmin[0] <= p.tau;       // guard band: the FP64 pass redoes this step
+            if (tid == 0) sp.flag[s] = redo ? 1 : 0;
+            if (redo) { __syncthreads(); continue; }
+        } else {
+            if (sp.pass == 1 && tid == 0) sp.flag[s] = 0;
+        }
+        if (tid == 0) p.rows[s * p.n_stride + (k - 1)] = sm.rows[k - 1];
+        const int nk = p.nk ? p.nk[s] : p.n_stride;
+        if (p.occ && k == nk) {
+            for (int rho = tid; rho < p.occ_stride; rho += blockDim.x) {
+                int c = 0;
+                for (int j = 0; j < k; ++j) c += (sm.rows[j] == rho) ? 1 : 0;
+                p.occ[s * (int64_t)p.occ_stride + rho] = c;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // Cofactors of S independent blocks: A [S][m][K] row-major, rows [S][K - 1].
 template <int TPL, int KPM, bool MIXED>
 __global__ void __launch_bounds__(256) cofactor_kernel(const double2* __restrict__ A, const int64_t* __restrict__ rows,
@@ -890,7 +1016,7 @@ __global__ void __launch_bounds__(256) cofactor_kernel(const double2* __restrict
     Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
     const int tid = threadIdx.x;
     for (int64_t s = blockIdx.x; s < S; s += gridDim.x) {
-        if (tid == 0) { sm.bad = 0; sm.ngrp = 0; }
+        if (tid == 0) { sm.bad = 0; sm.ngrp = 0; sm.lane0 = 0; sm.lane_mult = 1; }
         __syncthreads();
         if (tid < K) sm.cols[tid] = tid;
         if (tid < K - 1) {

@@ -98,6 +98,8 @@ struct Smem {
     int gmul[MAXN];                // their multiplicities
     int ngrp;
     int64_t cur;                   // stream being processed (-1: queue drained)
+    int64_t lane0;                 // this CTA's first Gray lane (split steps: chunk * lanes)
+    int lane_mult;                 // CTAs sharing one step of a stream (1 unless the step is split)
     double tot, target;
     int bad;                       // set by any thread that saw an out-of-range index
 };

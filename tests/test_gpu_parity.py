@@ -246,3 +246,32 @@ def test_an_out_of_range_column_is_reported_not_faulted():
         chain(acol, off, mm, nn, torch.zeros(2, dtype=torch.int64, device=DEV), cols, seeds=[1, 2, 3])
     rows, _, _ = chain(acol, off, mm, nn, torch.zeros(1, dtype=torch.int64, device=DEV), cols[:1], seeds=[1, 2, 3])
     assert rows.shape == (1, 3)
+
+
+# ------------------------------------------------------------------------------------------- split steps
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+@pytest.mark.parametrize("k_split,nch", [(2, 1), (6, 3), (9, 16), (12, 64)])
+def test_split_steps_match_single_cta_chains(precision, k_split, nch):
+    """Heavy steps shared by nch CTAs per stream give the single-CTA chains (FP64 marginals within 1e-12)."""
+    n, m, S = 14, 48, 6
+    U, sig, u = _random_chains(n, m, S, 31)
+    Ut = torch.tensor(U, device=DEV)
+    a = sample_chains(Ut, list(range(n)), sig, uniforms=u, want_marg=True, precision=precision, split=False)
+    b = sample_chains(Ut, list(range(n)), sig, uniforms=u, want_marg=True, precision=precision, split=(k_split, nch))
+    assert torch.equal(a["rows"], b["rows"]) and torch.equal(a["occ"], b["occ"])
+    ma, mb = a["marg"].cpu().numpy(), b["marg"].cpu().numpy()
+    for s in range(S):
+        for k in range(n):
+            tol = 1e-12 if precision == "f64" else mixed_tol(k + 1)      # FP32 blocks start at other lanes
+            assert _rel(mb[s, k], ma[s, k]) <= tol
+
+
+def test_single_sample_uses_the_whole_gpu_and_matches_the_oracle():
+    n, m = 18, 40
+    U, sig, u = _random_chains(n, m, 1, 41)
+    ref = O.chain(U[:, :n], np.zeros(1, np.int64), sig, u)
+    out = sample_chains(torch.tensor(U, device=DEV), list(range(n)), sig, uniforms=u, split=None)
+    assert np.array_equal(out["rows"].cpu().numpy(), ref["rows"])
+    occ = fock_sample(torch.tensor(U, device=DEV), list(range(n)), 1, generator=torch.Generator(device=DEV).manual_seed(2))
+    assert int(occ.sum()) == n
