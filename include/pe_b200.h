@@ -101,6 +101,21 @@ int pe_fock_chain_split(int precision, const double* d_acol, const int64_t* d_in
                         int marg_stride, int k_split, int nch, void* d_workspace, size_t workspace_bytes,
                         int block_threads, int tpl, void* stream);
 
+/*
+ * The same chains in the warp-per-stream form, for short chains (n_stride <= 16): every warp of a CTA
+ * runs its own stream (8 per CTA), so thousands of short chains progress at once without CTA-wide
+ * barriers.  Same algorithm, draws and rules; workspace as pe_fock_chain; tpl 1 or 2 (0 = default).
+ * Replaces, for small n, the launch-bound per-step loop of photonic_engines/clifford/sampler.py:420-456
+ * (two or three launches per step, cofactors_triton.py:368-391 for K1 <= 10).
+ */
+int pe_fock_chain_warp(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
+                       const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
+                       const int32_t* d_nk, const int64_t* d_cols, int n_stride, const double* d_uniforms,
+                       const int64_t* d_seeds, const int64_t* d_seed_row, const int64_t* d_rng_off,
+                       const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
+                       int marg_stride, void* d_workspace, size_t workspace_bytes, int tpl, int grid_ctas,
+                       void* stream);
+
 /* Bytes of device workspace pe_fock_chain_split needs for S streams and nch CTAs per stream. */
 size_t pe_chain_split_workspace_bytes(int64_t S, int nch);
 

@@ -12,6 +12,7 @@ import os
 
 import torch
 
+WARP_CANDIDATES = [(1, 256), (2, 256)]          # the warp form: threads per lane; the CTA is 8 warps
 CANDIDATES = {8: [(1, 128), (1, 256), (2, 128), (2, 256)],
               16: [(1, 128), (2, 128), (2, 256), (4, 256)],
               20: [(2, 128), (2, 256), (4, 128), (4, 256)],
@@ -61,14 +62,15 @@ def lookup(device, precision: str, workload: str):
     return tuple(hit) if hit else None
 
 
-def tune(run, device, precision: str, n_tier: int, workload: str, reps: int = 2, force: bool = False):
+def tune(run, device, precision: str, n_tier: int, workload: str, reps: int = 2, force: bool = False,
+         candidates=None):
     """run(tpl, block) performs one launch on the current stream.  Returns the fastest (tpl, block)."""
     k = key(device, precision, workload)
     cache = _load()
     if not force and k in cache:
         return tuple(cache[k])
     best, best_ms = None, float("inf")
-    for tpl, block in CANDIDATES[n_tier]:
+    for tpl, block in (candidates or CANDIDATES[n_tier]):
         run(tpl, block)                                         # warm-up (module load, attribute set-up)
         times = []
         for _ in range(reps):

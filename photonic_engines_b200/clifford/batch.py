@@ -19,7 +19,7 @@ import torch
 
 from .. import _native as N
 from .. import autotune
-from .kernels import pack_ragged, split_plan
+from .kernels import pack_ragged, split_plan, use_warp_form
 
 
 def _per_instance(v, G, default):
@@ -93,7 +93,8 @@ class BatchedSampler:
         self.rows = torch.zeros(C, ns, dtype=torch.int64, device=dev)
         self.occ = torch.zeros(S, self.m_max, dtype=torch.int64, device=dev)
         self.status = torch.zeros(2, dtype=torch.int32, device=dev)
-        self.split = split_plan(self.S, self.n_stride, dev, 256, 2)      # few long chains: share their steps
+        self.warp = use_warp_form(self.S, self.n_stride, dev)           # short chains: one warp per stream
+        self.split = None if self.warp else split_plan(self.S, self.n_stride, dev, 256, 2)   # few long chains
         if self.split:
             self.ws = torch.empty(int(N.load().pe_chain_split_workspace_bytes(C, self.split[1])), dtype=torch.uint8,
                                   device=dev)
@@ -134,7 +135,9 @@ class BatchedSampler:
                   self.m_max, None, self.m_max)
         block = int(self.block if block is None else block)
         tpl = int(self.tpl if tpl is None else tpl)
-        if self.split:
+        if self.warp:
+            rc = L.pe_fock_chain_warp(*common, N.ptr(self.ws), self.ws.numel(), tpl if tpl in (1, 2) else 0, 0, st)
+        elif self.split:
             rc = L.pe_fock_chain_split(*common, self.split[0], self.split[1], N.ptr(self.ws), self.ws.numel(), block,
                                        tpl, st)
         else:
@@ -154,11 +157,13 @@ class BatchedSampler:
         self._scatter()
 
     def _autotune(self):
-        workload = f"batch|G{self.G}|S{self.S}|m{self.m_max}|n{self.n_stride}|singles{int(self.singles)}"
+        workload = (f"batch|G{self.G}|S{self.S}|m{self.m_max}|n{self.n_stride}|singles{int(self.singles)}|"
+                    f"{'warp' if self.warp else 'cta'}")
         self._draw_keys()
         self._partition()
         best = autotune.tune(lambda tpl, block: self._chains(tpl, block), self.device, self.precision,
-                             autotune.tier(self.n_stride), workload)
+                             autotune.tier(self.n_stride), workload,
+                             candidates=autotune.WARP_CANDIDATES if self.warp else None)
         self.tpl, self.block = best
 
     def _capture(self):

@@ -71,17 +71,29 @@ def split_plan(heavy_streams: int, n: int, device, block_threads: int = 256, tpl
     return (k, nch) if k <= n else None
 
 
+WARP_MAX_PHOTONS = 16
+
+
+def use_warp_form(S: int, n: int, device) -> bool:
+    """The warp-per-stream form for short chains: always up to 12 photons, up to 16 when the streams are
+    many enough to fill the GPU's warps."""
+    if n > WARP_MAX_PHOTONS:
+        return False
+    return n <= 12 or S >= 64 * torch.cuda.get_device_properties(device).multi_processor_count
+
+
 def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst_n: torch.Tensor, dp, cols, *,
           m_max: int | None = None, nk=None, uniforms=None, seeds=None, seed_row=None, rng_off=None, order=None,
           want_occ: bool = True, occ_stride: int | None = None, want_marg: bool = False, precision: str = "f64",
           block_threads: int = 0, tpl: int = 0, grid_ctas: int = 0, check_status: bool = True, out=None,
-          split=None):
+          split=None, mode: str = "auto"):
     """Run the chains of S streams.  dp [S] instance per stream, cols [S, n_stride] input columns in chain order,
     nk [S] photons per stream (None: n_stride), uniforms [S, n_stride] (None: Philox from seeds [R, n_stride],
     seed_row [S], rng_off [S]).  Returns (rows [S, n_stride] int64, occ [S, occ_stride] or None,
     marg [S, n_stride, m_max] or None).  `out` may hold preallocated (rows, occ, marg) tensors.
     split: (k_split, nch) spreads every step k >= k_split over nch CTAs per stream (few-stream batches);
-    None or False runs each stream in one CTA."""
+    None or False runs each stream in one CTA.  mode: "cta" (one CTA per stream), "warp" (one warp per
+    stream, n_stride <= 16) or "auto" (warp form for short chains, see use_warp_form)."""
     N.require_cuda(acol, "acol")
     dev = acol.device
     L = N.load()
@@ -115,7 +127,15 @@ def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst
               int(m_max), int(S), N.ptr(dp), N.ptr(nk_t), N.ptr(cols), int(n_stride), N.ptr(u_t), N.ptr(seeds_t),
               N.ptr(_i64(seed_row, dev)), N.ptr(_i64(rng_off, dev)), N.ptr(_i64(order, dev)), N.ptr(rows), N.ptr(occ),
               int(occ_stride), N.ptr(marg), int(m_max))
-    if split:
+    if mode not in ("auto", "cta", "warp"):
+        raise ValueError(f"unknown mode {mode!r}: 'auto', 'cta' or 'warp'")
+    warp = (mode == "warp") or (mode == "auto" and not split and use_warp_form(S, n_stride, dev))
+    if warp:
+        ws = N.workspace(dev)
+        rc = L.pe_fock_chain_warp(*common, N.ptr(ws), int(ws.numel()), int(tpl if tpl in (1, 2) else 0),
+                                  int(grid_ctas), N.stream_handle(dev))
+        N.check(rc, "pe_fock_chain_warp")
+    elif split:
         k_split, nch = split
         ws = torch.empty(int(L.pe_chain_split_workspace_bytes(S, nch)), dtype=torch.uint8, device=dev)
         rc = L.pe_fock_chain_split(*common, int(k_split), int(nch), N.ptr(ws), int(ws.numel()), int(block_threads),

@@ -61,12 +61,12 @@ def _pass_draws(S: int, k: int, generator, dev, max_streams: int):
 
 def sample_chains(U, in_modes, sigma, *, uniforms=None, seeds=None, seed_row=None, rng_off=None, dp=None,
                   precision: str = "f64", want_marg: bool = False, block_threads: int = 0, tpl: int = 0,
-                  grid_ctas: int = 0, split=False):
+                  grid_ctas: int = 0, split=False, mode: str = "auto"):
     """The chains of S streams with a GIVEN column order: sigma [S, n] (indices into in_modes), per-step
     uniforms [S, n] (or the reference's Philox draws from seeds [n] / [R, n]).  dp [S]: circuit of each stream
     (default: all circuit 0 when U is [m, m], else b * shots layout is the caller's).
     split: False (one CTA per stream), None (spread heavy steps over several CTAs when the streams are too
-    few to fill the GPU) or an explicit (k_split, nch).
+    few to fill the GPU) or an explicit (k_split, nch).  mode: "auto" | "cta" | "warp" (kernels.chain).
     Returns dict(rows [S, n] ordered output modes, occ [S, m], marg [S, n, m] or None)."""
     N.require_cuda(U, "U")
     if U.dim() == 2:
@@ -82,7 +82,7 @@ def sample_chains(U, in_modes, sigma, *, uniforms=None, seeds=None, seed_row=Non
     rows, occ, marg = chain(acol, inst_off, inst_m, inst_n, dp, sigma, uniforms=uniforms, seeds=seeds,
                             seed_row=seed_row, rng_off=rng_off, want_occ=True, want_marg=want_marg,
                             precision=precision, block_threads=block_threads, tpl=tpl, grid_ctas=grid_ctas,
-                            split=split)
+                            split=split, mode=mode)
     return {"rows": rows, "occ": occ, "marg": marg}
 
 

@@ -7,6 +7,7 @@
 
 #include "fock_kernels.cuh"
 #include "fock_registry.h"
+#include "fock_warp.cuh"
 
 namespace pe {
 
@@ -26,11 +27,13 @@ static void* g_chain[2][3][N_KPM];
 static void* g_cof[2][3][N_KPM];
 static void* g_split_partial[2][3][N_KPM];
 static void* g_split_draw[2][N_KPM];
+static void* g_warp[2][3][N_KPM];
 
 void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cofactor_kernel, void* split_partial,
-                      void* split_draw) {
+                      void* split_draw, void* warp_kernel) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
     if (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) return;
+    g_warp[mixed][ti][ki] = warp_kernel;
     g_chain[mixed][ti][ki] = chain_kernel;
     g_cof[mixed][ti][ki] = cofactor_kernel;
     g_split_partial[mixed][ti][ki] = split_partial;
@@ -40,6 +43,11 @@ void* find_split_partial_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
     return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_split_partial[mixed][ti][ki];
 }
+void* find_warp_kernel(int mixed, int tpl, int kpm) {
+    const int ti = tpl_index(tpl), ki = kpm_index(kpm);
+    return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_warp[mixed][ti][ki];
+}
+size_t warp_smem_bytes() { return sizeof(WarpSmem) * WARPS; }
 void* find_split_draw_kernel(int mixed, int kpm) {
     const int ki = kpm_index(kpm);
     return (mixed < 0 || mixed > 1 || ki < 0) ? nullptr : g_split_draw[mixed][ki];
@@ -139,7 +147,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
                         const int64_t* d_seeds, const int64_t* d_seed_row, const int64_t* d_rng_off,
                         const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
                         int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
-                        int grid_ctas, int k_split, int nch, void* stream) {
+                        int grid_ctas, int k_split, int nch, void* stream, bool warp_mode = false) {
     if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
     if (S < 0 || G < 1 || m_max < 1 || n_stride < 1) return PE_ERR_ARG;
     if (!d_acol || !d_inst_off || !d_inst_m || !d_inst_n || !d_dp || !d_cols || !d_rows || !d_workspace) return PE_ERR_ARG;
@@ -153,13 +161,14 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     if (workspace_bytes < need || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
     const int kpm = kpm_for(n_stride);
     if (kpm < 0) return PE_ERR_SIZE;
-    if (tpl == 0) tpl = default_tpl(kpm);
+    if (warp_mode && (kpm > WMAXN || split)) return PE_ERR_SIZE;
+    if (tpl == 0) tpl = warp_mode ? (kpm <= 8 ? 1 : 2) : default_tpl(kpm);
     if (tpl_index(tpl) < 0) return PE_ERR_ARG;
-    void* fn = find_chain_kernel(precision, tpl, kpm);
+    void* fn = warp_mode ? find_warp_kernel(precision, tpl, kpm) : find_chain_kernel(precision, tpl, kpm);
     if (!fn) return PE_ERR_SIZE;
-    const int block = block_threads ? block_threads : 256;
+    const int block = warp_mode ? 32 * WARPS : (block_threads ? block_threads : 256);
     if (block < 32 || block > 256 || (block & 31)) return PE_ERR_ARG;
-    const size_t smem = smem_fixed_bytes() + (size_t)m_max * sizeof(double);
+    const size_t smem = warp_mode ? warp_smem_bytes() : smem_fixed_bytes() + (size_t)m_max * sizeof(double);
     const int cap = max_smem_optin();
     if (cap <= 0) return PE_ERR_CUDA;
     if (smem > (size_t)cap) return PE_ERR_SIZE;
@@ -173,7 +182,8 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int64_t grid = grid_ctas > 0 ? grid_ctas : (int64_t)sms * per_sm;
-    if (grid > S) grid = S;
+    const int64_t units = warp_mode ? (S + WARPS - 1) / WARPS : S;      // streams in flight per CTA
+    if (grid > units) grid = units;
     if (grid < 1) grid = 1;
     ChainParams p;
     p.acol = (const double2*)d_acol;
@@ -234,6 +244,18 @@ extern "C" int pe_fock_chain(int precision, const double* d_acol, const int64_t*
     return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, d_nk, d_cols, n_stride,
                         d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ, occ_stride, d_marg,
                         marg_stride, d_workspace, workspace_bytes, block_threads, tpl, grid_ctas, 0, 1, stream);
+}
+
+extern "C" int pe_fock_chain_warp(int precision, const double* d_acol, const int64_t* d_inst_off,
+                                  const int32_t* d_inst_m, const int32_t* d_inst_n, int G, int m_max, int64_t S,
+                                  const int64_t* d_dp, const int32_t* d_nk, const int64_t* d_cols, int n_stride,
+                                  const double* d_uniforms, const int64_t* d_seeds, const int64_t* d_seed_row,
+                                  const int64_t* d_rng_off, const int64_t* d_order, int64_t* d_rows, int64_t* d_occ,
+                                  int occ_stride, double* d_marg, int marg_stride, void* d_workspace,
+                                  size_t workspace_bytes, int tpl, int grid_ctas, void* stream) {
+    return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, d_nk, d_cols, n_stride,
+                        d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ, occ_stride, d_marg,
+                        marg_stride, d_workspace, workspace_bytes, 0, tpl, grid_ctas, 0, 1, stream, true);
 }
 
 extern "C" size_t pe_chain_split_workspace_bytes(int64_t S, int nch) {

@@ -3,6 +3,7 @@
 // per variant, in parallel, and links the objects into one library.
 #include "fock_kernels.cuh"
 #include "fock_registry.h"
+#include "fock_warp.cuh"
 
 #if !defined(PE_MIXED) || !defined(PE_TPL) || !defined(PE_KPM)
 #error "PE_MIXED, PE_TPL and PE_KPM must be defined"
@@ -15,7 +16,13 @@ struct Registration {
                              (void*)pe::fock_chain_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
                              (void*)pe::cofactor_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
                              (void*)pe::split_partial_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
-                             (void*)pe::split_draw_kernel<PE_KPM, (PE_MIXED != 0)>);
+                             (void*)pe::split_draw_kernel<PE_KPM, (PE_MIXED != 0)>,
+#if PE_KPM <= 16 && PE_TPL <= 2
+                             (void*)pe::fock_chain_warp_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>
+#else
+                             nullptr
+#endif
+        );
     }
 };
 Registration registration;

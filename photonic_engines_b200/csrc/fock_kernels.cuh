@@ -87,7 +87,8 @@ static __device__ __forceinline__ void record_error(int* status, long long* deta
 // ---------------------------------------------------------------------------------------- groups
 // Thread 0, after every pick: the distinct chosen modes and their multiplicities (the grouping of
 // cofactors_triton.py:419-427, kept incrementally instead of re-sorting the rows every step).
-static __device__ __forceinline__ void add_to_groups(Smem& sm, int row) {
+template <class SM>
+__device__ __forceinline__ void add_to_groups(SM& sm, int row) {
     for (int g = 0; g < sm.ngrp; ++g)
         if (sm.grow[g] == row) { sm.gmul[g] += 1; return; }
     sm.grow[sm.ngrp] = row;
@@ -102,7 +103,8 @@ static __device__ __forceinline__ void add_to_groups(Smem& sm, int row) {
 // change N or the sum.  Active digits (radix >= 2) are ranked by ascending radix; the leading ones
 // become the Gray lanes (best fill of the CTA's lanes), the next ones the inner block, then the
 // middle block; what does not fit the schedules joins the lanes.
-static __device__ void plan_step(Smem& sm, int K1, int K, int lanes, int lin_max) {
+template <class SM>
+__device__ void plan_step(SM& sm, int K1, int K, int lanes, int lin_max, int mid_max) {
     Plan& pl = sm.plan;
     const int lane = threadIdx.x & 31;
     const int D = sm.ngrp;
@@ -143,7 +145,7 @@ static __device__ void plan_step(Smem& sm, int K1, int K, int lanes, int lin_max
         int nin = 0, Lin = 1;
         while (nhi + nin < na && Lin * pl.sortR[nhi + nin] <= lin_max) { Lin *= pl.sortR[nhi + nin]; ++nin; }
         int nmid = 0, Lmid = 1;
-        while (nhi + nin + nmid < na && Lmid * pl.sortR[nhi + nin + nmid] <= MID_MAX) {
+        while (nhi + nin + nmid < na && Lmid * pl.sortR[nhi + nin + nmid] <= mid_max) {
             Lmid *= pl.sortR[nhi + nin + nmid];
             ++nmid;
         }
@@ -480,9 +482,9 @@ __device__ __forceinline__ void term2(R (&sr)[KH], R (&si)[KH], R (&ar)[KH], R (
 
 // Walk one inner block forward (fwd) or backward from the current column sums.  `f2` is the
 // magnitude of the column-sum step (2 for B, 1 for the pre-doubled B32); w_t = wscale * tab[t].
-template <int KH, int TPL, int UNR, typename R, typename C2, typename TabW>
-__device__ __forceinline__ void inner_block(R (&sr)[KH], R (&si)[KH], R (&ar)[KH], R (&ai)[KH], const Smem& sm,
-                                           const C2 (*Bm)[MAXN], const TabW* tab, R wscale, R f2, bool fwd, int Lin,
+template <int KH, int TPL, int UNR, typename R, typename C2, typename TabW, class SM, class BMat>
+__device__ __forceinline__ void inner_block(R (&sr)[KH], R (&si)[KH], R (&ar)[KH], R (&ai)[KH], const SM& sm,
+                                           const BMat& Bm, const TabW* tab, R wscale, R f2, bool fwd, int Lin,
                                            int c0, int h, unsigned gmask) {
     if (fwd) {
         term_any<KH, TPL, R, C2>(sr, si, ar, ai, nullptr, R(0), wscale * (R)tab[0], h, gmask);
@@ -561,8 +563,8 @@ static __device__ __forceinline__ uint64_t lane_digits(const Plan& pl, int64_t h
 // Column sums of one lane at a given digit state, FP64: s_j = sum_kd (M_kd - 2 v_kd) B[kd][j] with the
 // inner digits at their start (0) or end (vend) state, the middle digits at middle index pm and the
 // high digits of the lane (packed by lane_digits; more than 12 high digits are decoded from hl).
-template <int KH>
-__device__ __forceinline__ void lane_sums(const Smem& sm, int c0, bool inner_end, int pm, int64_t hl, uint64_t hpack,
+template <int KH, class SM>
+__device__ __forceinline__ void lane_sums(const SM& sm, int c0, bool inner_end, int pm, int64_t hl, uint64_t hpack,
                                           double (&xr)[KH], double (&xi)[KH]) {
     const Plan& pl = sm.plan;
 #pragma unroll
@@ -709,7 +711,7 @@ __device__ void dispatch_mixed(Smem& sm, int K) {
 // One cofactor step of the stream held in shared memory (K1 >= 1): plan, prepare, sweep.
 template <int TPL, int KPM, bool MIXED>
 __device__ __forceinline__ void cofactor_step(Smem& sm, const double2* A, int64_t rs, int64_t cs, int K1, int K) {
-    if (threadIdx.x < 32) plan_step(sm, K1, K, blockDim.x / TPL * sm.lane_mult, MIXED ? MIXED_LIN : LIN_MAX);
+    if (threadIdx.x < 32) plan_step(sm, K1, K, blockDim.x / TPL * sm.lane_mult, MIXED ? MIXED_LIN : LIN_MAX, MID_MAX);
     __syncthreads();
     prepare_step(sm, A, rs, cs, MIXED);
     __syncthreads();

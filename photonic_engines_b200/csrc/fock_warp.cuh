@@ -1,0 +1,321 @@
+// Warp-per-stream form of the chain kernel, for short chains (at most 16 photons): every warp of a CTA
+// runs its own stream, so the per-step work (plan, schedules, draw) of many streams proceeds at once
+// and nothing waits on a CTA-wide barrier.  Same algorithm, plan, Gray schedules, all-but-one products,
+// draw rule and uniforms as the CTA form (fock_kernels.cuh); the lanes of the collapsed sum are the
+// warp's 32 / TPL thread groups.  The marginal's CDF is formed in 32-mode chunks twice (once for the
+// total, once for the pick) instead of being stored, so any number of modes fits.
+#pragma once
+#include "fock_kernels.cuh"
+
+namespace pe {
+
+constexpr int WMAXN = 16;      // photons per stream
+constexpr int WLIN = 128;      // inner schedule length
+constexpr int WMID = 128;      // middle schedule length
+constexpr int WARPS = 8;       // warps (streams in flight) per CTA
+
+struct WarpSmem {
+    Plan plan;
+    double2 P[WMAXN];
+    double2 B[WMAXN][WMAXN];
+    float2 B32[WMAXN][WMAXN];
+    double tab_w[WLIN];
+    float tab_w32[WLIN];
+    double tab_wm[WMID];
+    unsigned char tab_f[WLIN];
+    unsigned char tab_fm[WMID];
+    int rows[WMAXN];
+    int cols[WMAXN];
+    int grow[WMAXN];
+    int gmul[WMAXN];
+    int ngrp;
+    int bad;
+    int64_t cur;
+    int64_t lane0;
+    int lane_mult;
+};
+
+// Gather B and fill the schedules, lane-parallel.  Element (rho, j) of the instance is A[rho + j * m].
+static __device__ void prepare_warp(WarpSmem& sm, const double2* __restrict__ A, int m, bool mixed) {
+    const Plan& pl = sm.plan;
+    const int lane = threadIdx.x & 31;
+    for (int idx = lane; idx < pl.D * WMAXN; idx += 32) {
+        const int kd = idx / WMAXN, j = idx % WMAXN;
+        double2 b = make_double2(0.0, 0.0);
+        if (j < pl.K) b = A[(int64_t)pl.drow[kd] + (int64_t)sm.cols[j] * m];
+        sm.B[kd][j] = b;
+        if (mixed) sm.B32[kd][j] = make_float2((float)(2.0 * b.x), (float)(2.0 * b.y));
+    }
+    for (int t = lane; t < pl.Lin; t += 32) {
+        double w;
+        sm.tab_f[t] = gray_entry(pl, 0, pl.nin, pl.Pin, t, &w, t == pl.Lin - 1 ? sm.plan.vend : nullptr);
+        sm.tab_w[t] = w;
+        sm.tab_w32[t] = (float)w;
+    }
+    for (int t = lane; t < pl.Lmid; t += 32) {
+        double w;
+        sm.tab_fm[t] = gray_entry(pl, pl.nin, pl.nmid, pl.Pmid, t, &w, nullptr);
+        sm.tab_wm[t] = w;
+    }
+}
+
+// Sum of the warp's lane accumulators (all lanes of a thread position hold the same total), times the
+// scale, into sm.P.
+template <int KH, int TPL>
+__device__ __forceinline__ void reduce_warp_to_P(double (&ar)[KH], double (&ai)[KH], WarpSmem& sm, int c0) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < KH; ++j) {
+#pragma unroll
+        for (int o = TPL; o < 32; o <<= 1) {
+            ar[j] += __shfl_xor_sync(0xffffffffu, ar[j], o);
+            ai[j] += __shfl_xor_sync(0xffffffffu, ai[j], o);
+        }
+    }
+    if (lane < TPL) {
+#pragma unroll
+        for (int j = 0; j < KH; ++j)
+            if (c0 + j < sm.plan.K) sm.P[c0 + j] = make_double2(ar[j] * sm.plan.scale, ai[j] * sm.plan.scale);
+    }
+    __syncwarp();
+}
+
+template <int KP, int TPL>
+__device__ void sweep_warp_f64(WarpSmem& sm) {
+    constexpr int KH = KP / TPL;
+    const Plan& pl = sm.plan;
+    const int lane_id = threadIdx.x & 31;
+    const int lanes = 32 / TPL, lane = lane_id / TPL, h = lane_id % TPL, c0 = h * KH;
+    const unsigned gmask = group_mask<TPL>();
+    const int K = pl.K, Lin = pl.Lin, Lmid = pl.Lmid, nin = pl.nin;
+    const int64_t H = pl.H;
+    double ar[KH], ai[KH];
+#pragma unroll
+    for (int j = 0; j < KH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
+    for (int64_t hl = lane; hl < H; hl += lanes) {
+        double sr[KH], si[KH], wh;
+        const uint64_t hpack = lane_digits(pl, hl, &wh);
+        lane_sums<KH>(sm, c0, false, 0, hl, hpack, sr, si);
+#pragma unroll
+        for (int j = 0; j < KH; ++j) if (c0 + j >= K) { sr[j] = 1.0; si[j] = 0.0; }
+        for (int pm = 0; pm < Lmid; ++pm) {
+            if (pm > 0) {
+                const unsigned e = sm.tab_fm[pm];
+                const double f = (e & 0x80u) ? -2.0 : 2.0;
+                const double2* b = &sm.B[nin + (e & 63u)][c0];
+#pragma unroll
+                for (int j = 0; j < KH; ++j) { sr[j] = fma(f, b[j].x, sr[j]); si[j] = fma(f, b[j].y, si[j]); }
+            }
+            const double wmh = wh * sm.tab_wm[pm];
+            inner_block<KH, TPL, 1, double, double2, double>(sr, si, ar, ai, sm, sm.B, sm.tab_w, wmh, 2.0, !(pm & 1),
+                                                             Lin, c0, h, gmask);
+        }
+    }
+    reduce_warp_to_P<KH, TPL>(ar, ai, sm, c0);
+}
+
+template <int KP, int TPL>
+__device__ void sweep_warp_mixed(WarpSmem& sm) {
+    constexpr int KH = KP / TPL;
+    const Plan& pl = sm.plan;
+    const int lane_id = threadIdx.x & 31;
+    const int lanes = 32 / TPL, lane = lane_id / TPL, h = lane_id % TPL, c0 = h * KH;
+    const unsigned gmask = group_mask<TPL>();
+    const int K = pl.K, Lin = pl.Lin, Lmid = pl.Lmid;
+    const int64_t H = pl.H;
+    double ar[KH], ai[KH];
+#pragma unroll
+    for (int j = 0; j < KH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
+    for (int64_t hl = lane; hl < H; hl += lanes) {
+        double wh;
+        const uint64_t hpack = lane_digits(pl, hl, &wh);
+        for (int pm = 0; pm < Lmid; ++pm) {
+            const bool fwd = !(pm & 1);
+            float sr[KH], si[KH];
+            {
+                double xr[KH], xi[KH];
+                lane_sums<KH>(sm, c0, !fwd, pm, hl, hpack, xr, xi);
+#pragma unroll
+                for (int j = 0; j < KH; ++j) {
+                    const bool pad = c0 + j >= K;
+                    sr[j] = pad ? 1.0f : (float)xr[j];
+                    si[j] = pad ? 0.0f : (float)xi[j];
+                }
+            }
+            float a32r[KH], a32i[KH];
+#pragma unroll
+            for (int j = 0; j < KH; ++j) { a32r[j] = 0.0f; a32i[j] = 0.0f; }
+            inner_block<KH, TPL, 1, float, float2, float>(sr, si, a32r, a32i, sm, sm.B32, sm.tab_w32, 1.0f, 1.0f, fwd,
+                                                          Lin, c0, h, gmask);
+            const double wmh = wh * sm.tab_wm[pm];
+#pragma unroll
+            for (int j = 0; j < KH; ++j) { ar[j] = fma(wmh, (double)a32r[j], ar[j]); ai[j] = fma(wmh, (double)a32i[j], ai[j]); }
+        }
+    }
+    reduce_warp_to_P<KH, TPL>(ar, ai, sm, c0);
+}
+
+#define PE_WTIER(KPv, CALL)                                  \
+    if constexpr (KPW >= KPv) {                              \
+        if (K <= KPv) { CALL; return; }                      \
+    }
+
+template <int TPL, int KPW, bool MIXED>
+__device__ void warp_cofactors(WarpSmem& sm, int K) {
+    if constexpr (MIXED) {
+        PE_WTIER(4, (sweep_warp_mixed<4, TPL>(sm)))
+        PE_WTIER(8, (sweep_warp_mixed<8, TPL>(sm)))
+        PE_WTIER(12, (sweep_warp_mixed<12, TPL>(sm)))
+        PE_WTIER(16, (sweep_warp_mixed<16, TPL>(sm)))
+    } else {
+        PE_WTIER(4, (sweep_warp_f64<4, TPL>(sm)))
+        PE_WTIER(8, (sweep_warp_f64<8, TPL>(sm)))
+        PE_WTIER(12, (sweep_warp_f64<12, TPL>(sm)))
+        PE_WTIER(16, (sweep_warp_f64<16, TPL>(sm)))
+    }
+}
+
+// Marginal, CDF and pick of one step (the rule of cofactors_triton.py:298-308, tot = cw[m - 1]); the
+// 32-mode chunks are scanned twice.  Returns min |cw - u tot| / tot.
+static __device__ double draw_warp(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
+                                   double* __restrict__ marg_row) {
+    const int lane = threadIdx.x & 31;
+    double tot = 0.0;
+    for (int pass = 0; pass < 2; ++pass) {
+        const double target = u * tot;
+        double carry = 0.0, gmin = 1.0e300;
+        int cnt = 0;
+        for (int base = 0; base < m; base += 32) {
+            const int rho = base + lane;
+            double w = 0.0;
+            if (rho < m) {
+                double xr = 0.0, xi = 0.0;
+                for (int c = 0; c < k; ++c) {
+                    const double2 a = A[(int64_t)rho + (int64_t)sm.cols[c] * m];
+                    const double2 p = sm.P[c];
+                    xr = fma(a.x, p.x, xr);
+                    xr = fma(-a.y, p.y, xr);
+                    xi = fma(a.x, p.y, xi);
+                    xi = fma(a.y, p.x, xi);
+                }
+                w = xr * xr + xi * xi;
+            }
+            double x = w;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            const double cw = carry + x;
+            if (pass == 1 && rho < m) {
+                cnt += (cw < target) ? 1 : 0;
+                gmin = fmin(gmin, fabs(cw - target));
+                if (marg_row) marg_row[rho] = w / tot;
+            }
+            carry = __shfl_sync(0xffffffffu, cw, 31);
+        }
+        if (pass == 0) {
+            tot = carry;
+        } else {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+                gmin = fmin(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
+            }
+            if (lane == 0) sm.rows[k - 1] = min(cnt, m - 1);
+            __syncwarp();
+            return gmin / tot;
+        }
+    }
+    return 0.0;
+}
+
+template <int TPL, int KPW, bool MIXED>
+__device__ void chain_warp(const ChainParams& p, WarpSmem& sm, int64_t s) {
+    const int lane = threadIdx.x & 31;
+    const int64_t g = p.dp[s];
+    bool ok = g >= 0 && g < p.G;
+    int m = 0, nin = 0;
+    int64_t off = 0;
+    if (ok) { m = p.inst_m[g]; nin = p.inst_n[g]; off = p.inst_off[g]; }
+    const int nk = p.nk ? p.nk[s] : p.n_stride;
+    ok = ok && nk >= 0 && nk <= p.n_stride && nk <= KPW && m >= 1 && m <= p.m_cap && m <= p.occ_stride;
+    bool badcol = false;
+    if (ok && lane < nk) {
+        const int64_t c = p.cols[s * p.n_stride + lane];
+        if (c < 0 || c >= nin) badcol = true;
+        else sm.cols[lane] = (int)c;
+    }
+    if (!ok || __any_sync(0xffffffffu, badcol)) {
+        if (lane == 0) record_error(p.status, p.detail, s);
+        __syncwarp();
+        return;
+    }
+    if (lane == 0) { sm.ngrp = 0; sm.lane0 = 0; sm.lane_mult = 1; }
+    __syncwarp();
+    const double2* A = p.acol + off;
+    for (int k = 1; k <= nk; ++k) {
+        const int K1 = k - 1;
+        if (K1 == 0) {
+            if (lane == 0) sm.P[0] = make_double2(1.0, 0.0);
+            __syncwarp();
+        } else {
+            plan_step(sm, K1, k, 32 / TPL, WLIN, WMID);
+            __syncwarp();
+            prepare_warp(sm, A, m, MIXED);
+            __syncwarp();
+            warp_cofactors<TPL, KPW, MIXED>(sm, k);
+        }
+        double u;
+        if (p.uniforms) {
+            u = p.uniforms[s * p.n_stride + (k - 1)];
+        } else {
+            const int64_t row = p.seed_row ? p.seed_row[s] : 0;
+            const int64_t ro = p.rng_off ? p.rng_off[s] : s;
+            u = chain_uniform((uint64_t)p.seeds[row * p.n_stride + (k - 1)], ro);
+        }
+        double* mrow = p.marg ? p.marg + ((size_t)s * p.n_stride + (k - 1)) * p.marg_stride : nullptr;
+        const double gap = draw_warp(sm, A, m, k, u, mrow);
+        if constexpr (MIXED) {
+            if (K1 > 0 && gap <= p.tau) {                  // guard band: this step again in FP64
+                warp_cofactors<TPL, KPW, false>(sm, k);
+                draw_warp(sm, A, m, k, u, mrow);
+            }
+        }
+        if (lane == 0) add_to_groups(sm, sm.rows[k - 1]);
+        __syncwarp();
+    }
+    for (int j = lane; j < nk; j += 32) p.rows[s * p.n_stride + j] = sm.rows[j];
+    if (p.occ) {
+        for (int rho = lane; rho < p.occ_stride; rho += 32) {
+            int c = 0;
+            for (int j = 0; j < nk; ++j) c += (sm.rows[j] == rho) ? 1 : 0;
+            p.occ[s * (int64_t)p.occ_stride + rho] = c;
+        }
+    }
+    __syncwarp();
+}
+
+template <int TPL, int KPW, bool MIXED>
+__global__ void __launch_bounds__(32 * WARPS, 2) fock_chain_warp_kernel(ChainParams p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WarpSmem& sm = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        if (lane == 0) {
+            const unsigned long long q = atomicAdd(p.queue, 1ull);
+            sm.cur = (q < (unsigned long long)p.S) ? (p.order ? p.order[q] : (int64_t)q) : -1;
+        }
+        __syncwarp();
+        const int64_t s = sm.cur;
+        if (s < 0) return;
+        if (s >= p.S) {
+            if (lane == 0) record_error(p.status, p.detail, s);
+            return;
+        }
+        chain_warp<TPL, KPW, MIXED>(p, sm, s);
+    }
+}
+
+}  // namespace pe

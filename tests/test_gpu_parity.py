@@ -137,13 +137,14 @@ def _random_chains(n, m, S, seed):
     return U, sig, u
 
 
-@pytest.mark.parametrize("n,m,S", [(6, 12, 64), (12, 40, 32), (20, 400, 24)])
-def test_chains_match_the_oracle_with_supplied_uniforms(n, m, S):
+@pytest.mark.parametrize("n,m,S,mode", [(6, 12, 64, "cta"), (6, 12, 64, "warp"), (12, 40, 32, "cta"),
+                                        (12, 40, 32, "warp"), (16, 60, 24, "warp"), (20, 400, 24, "cta")])
+def test_chains_match_the_oracle_with_supplied_uniforms(n, m, S, mode):
     U, sig, u = _random_chains(n, m, S, 1000 + n)
     ref = O.chain(U[:, :n], np.zeros(S, np.int64), sig, u, marg=True)
     Ut = torch.tensor(U, device=DEV)
-    f64 = sample_chains(Ut, list(range(n)), sig, uniforms=u, want_marg=True)
-    mix = sample_chains(Ut, list(range(n)), sig, uniforms=u, want_marg=True, precision="mixed")
+    f64 = sample_chains(Ut, list(range(n)), sig, uniforms=u, want_marg=True, mode=mode)
+    mix = sample_chains(Ut, list(range(n)), sig, uniforms=u, want_marg=True, precision="mixed", mode=mode)
     rows64 = f64["rows"].cpu().numpy()
     far = (ref["gap"] > 1e-11).all(axis=1)
     assert far.mean() > 0.9
@@ -161,8 +162,21 @@ def test_launch_shapes_give_identical_picks(block, tpl):
     n, m, S = 10, 30, 40
     U, sig, u = _random_chains(n, m, S, 77)
     ref = O.chain(U[:, :n], np.zeros(S, np.int64), sig, u)
-    out = sample_chains(torch.tensor(U, device=DEV), list(range(n)), sig, uniforms=u, block_threads=block, tpl=tpl)
+    out = sample_chains(torch.tensor(U, device=DEV), list(range(n)), sig, uniforms=u, block_threads=block, tpl=tpl,
+                        mode="cta")
     assert np.array_equal(out["rows"].cpu().numpy(), ref["rows"])
+
+
+@pytest.mark.parametrize("tpl", [1, 2])
+@pytest.mark.parametrize("n,m", [(3, 5), (9, 30), (14, 100)])
+def test_warp_form_thread_groupings_give_identical_picks(tpl, n, m):
+    S = 80
+    U, sig, u = _random_chains(n, m, S, 55 + n)
+    ref = O.chain(U[:, :n], np.zeros(S, np.int64), sig, u)
+    for precision in ("f64", "mixed"):
+        out = sample_chains(torch.tensor(U, device=DEV), list(range(n)), sig, uniforms=u, tpl=tpl, mode="warp",
+                            precision=precision)
+        assert np.array_equal(out["rows"].cpu().numpy(), ref["rows"])
 
 
 # ------------------------------------------------------------------------------------------- distributions
