@@ -120,6 +120,33 @@ int pe_fock_chain_warp(int precision, const double* d_acol, const int64_t* d_ins
 size_t pe_chain_split_workspace_bytes(int64_t S, int nch);
 
 /*
+ * Adaptive chains: a forced prefix and an avoided set of output modes (photonic_engines/clifford/
+ * sampler.py:391-460, `_sample_streams(..., prefix=, avoid=)`, reached from fock_sample(prefix=, avoid=),
+ * sampler.py:57-182).  Every stream has n_stride photons (the reference allows prefix / avoid on lossless,
+ * indistinguishable photons only).  d_rows [S][n_stride]: on entry its first n_prefix entries per stream
+ * are the forced output modes; the chain runs steps n_prefix + 1 .. n_stride on the caller's column order
+ * d_cols (whose first n_prefix columns are the set drawn for the prefix).
+ * d_avoid (optional, uint8 [m_max], 1 = avoided mode): after every step past the first free one, a stream
+ * whose last row is avoided is dropped, and the survivors of each pass chunk are renumbered before the
+ * next step's draws exactly as the reference shrinks its batch (the Philox stream offset of a survivor is
+ * its rank among the chunk's survivors; chunk start = s - d_rng_off[s]); the row of the last step is
+ * checked too.  d_alive (uint8 [S], required with d_avoid): 1 for the streams that survived.  d_occ
+ * (optional [S][occ_stride]): occupations including the prefix; rows of dropped streams are zeroed.
+ * mode 0: one CTA per stream (k_split / nch as pe_fock_chain_split, or 0 / 0); mode 1: one warp per
+ * stream (n_stride <= 16, no split).  Workspace: pe_adaptive_workspace_bytes(S, nch) (nch 0 without a
+ * split).  With d_avoid the call is one launch per step plus a one-CTA survivor update between steps,
+ * all on `stream` (no host synchronisation); without it, one launch.  Other arguments as pe_fock_chain.
+ */
+int pe_fock_chain_adaptive(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
+                           const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
+                           const int64_t* d_cols, int n_stride, const double* d_uniforms, const int64_t* d_seeds,
+                           const int64_t* d_seed_row, const int64_t* d_rng_off, int64_t* d_rows, int n_prefix,
+                           const uint8_t* d_avoid, uint8_t* d_alive, int64_t* d_occ, int occ_stride, int k_split,
+                           int nch, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl, int mode,
+                           void* stream);
+size_t pe_adaptive_workspace_bytes(int64_t S, int nch);
+
+/*
  * pe_fock_chain without a workspace argument: the same chains and outputs, for callers that cannot
  * allocate device memory when they sample (a host callback or other context where CUDA allocation is not
  * allowed, a serving process whose device memory all belongs to its own arena, a foreign-language

@@ -11,6 +11,7 @@ What it restates (file:line in the reference project):
   2020 cofactors, exact all-but-one      photonic_engines/clifford/variants.py:70-114
   amplitudes, 48-bit uniform, pick rule  photonic_engines/clifford/cofactors_triton.py:287-308
   Philox4x32-10 as tl.rand calls it      triton/language/random.py (installed Triton)
+  forced prefix / avoided modes          photonic_engines/clifford/sampler.py:391-460 (adaptive_chains)
   Ryser permanent                        tests/clifford/check_cofactors.py:17-24
   exact output distribution              tests/clifford/check_sampler.py:25-37
   Haar unitary                           tests/helpers.py:10-17
@@ -173,6 +174,53 @@ def chain(A, dp, sigma, u, precision: str = "f64", marg: bool = False, threads: 
     if rc != 0:
         raise ValueError("oracle chain: bad sizes or instance ids")
     return {"rows": rows, "gap": gap, "addends": add, "marg": mg}
+
+
+def adaptive_chains(A, dp, sigma, prefix_rows, seeds, seed_row, rng_off0, avoid=None,
+                    precision: str = "f64") -> tuple[np.ndarray, np.ndarray]:
+    """Chains with a forced prefix and avoided modes, stream by stream in the reference's step order
+    (sampler.py:391-460): rows[:, :c] = prefix_rows, steps c + 1..n on the column order sigma [S, n];
+    with `avoid`, before every step after the first free one a stream whose last row is avoided is
+    dropped, and each pass chunk's survivors are renumbered (chunk start s - rng_off0[s]) before the next
+    step's draws, whose stream offset is that rank; the last row is checked after the last step.
+    A [G, m, n] complex, seeds [R, n], seed_row [S].  Returns (rows [S, n], alive [S] bool); a dropped
+    stream keeps the rows drawn up to its drop and -1 after it."""
+    A = _c128(A)
+    if A.ndim == 2:
+        A = A[None]
+    dp = np.asarray(dp, dtype=np.int64).reshape(-1)
+    S = dp.shape[0]
+    sigma = np.asarray(sigma, dtype=np.int64).reshape(S, -1)
+    n = sigma.shape[1]
+    pre = np.asarray(prefix_rows, dtype=np.int64).reshape(S, -1)
+    c0 = pre.shape[1]
+    seeds = np.asarray(seeds, dtype=np.int64).reshape(-1, n)
+    seed_row = np.asarray(seed_row, dtype=np.int64).reshape(-1)
+    off0 = np.asarray(rng_off0, dtype=np.int64).reshape(-1)
+    start = np.arange(S) - off0
+    avoid_set = set(int(r) for r in avoid) if avoid is not None else None
+    rows = np.full((S, n), -1, dtype=np.int64)
+    rows[:, :c0] = pre
+    alive = np.ones(S, dtype=bool)
+    L = lib()
+    for k in range(c0 + 1, n + 1):
+        if avoid_set is not None and k > c0 + 1:
+            alive = np.array([bool(alive[s]) and int(rows[s, k - 2]) not in avoid_set for s in range(S)])
+        rank = np.zeros(S, dtype=np.int64)
+        counts: dict = {}
+        for s in range(S):
+            if alive[s]:
+                rank[s] = counts.get(int(start[s]), 0)
+                counts[int(start[s])] = rank[s] + 1
+        for s in range(S):
+            if not alive[s]:
+                continue
+            u = L.oracle_uniform(int(seeds[seed_row[s], k - 1]), int(rank[s]))
+            idx, _, _ = step(A[dp[s]], rows[s, :k - 1], sigma[s, :k], u, precision)
+            rows[s, k - 1] = idx
+    if avoid_set is not None and n > c0:
+        alive = np.array([bool(alive[s]) and int(rows[s, n - 1]) not in avoid_set for s in range(S)])
+    return rows, alive
 
 
 def occupations(rows, m: int) -> np.ndarray:

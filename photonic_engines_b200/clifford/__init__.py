@@ -5,6 +5,8 @@
     sample_chains(U, in_modes, sigma, uniforms=...)                     chains with a given column order
     BatchedSampler(circuits, shots, loss=, indist=)                     many circuits, one launch, CUDA graph
     laplace_cofactors_rows(A, rows)                                     the cofactor step alone
+    prefix_columns(A, prefix, shots, generator), prefix_columns_many,  column sets for a forced prefix
+    prefix_subset_weights(A, prefix)                                    (adaptive sampling)
 
 Mirrors photonic_engines/clifford/__init__.py:139-166 for Fock inputs; other input types (emitter,
 superposition) are not part of this library and raise.
@@ -16,9 +18,11 @@ import torch
 from ..states import FockState
 from .batch import BatchedSampler
 from .kernels import laplace_cofactors_rows
+from .prefix import prefix_columns, prefix_columns_many, prefix_subset_weights
 from .sampler import fock_sample, sample_chains
 
-__all__ = ["BatchedSampler", "fock_sample", "laplace_cofactors_rows", "sample", "sample_chains"]
+__all__ = ["BatchedSampler", "fock_sample", "laplace_cofactors_rows", "prefix_columns", "prefix_columns_many",
+           "prefix_subset_weights", "sample", "sample_chains"]
 
 
 def sample(state, U: torch.Tensor, shots: int, generator: torch.Generator | None = None, **kw):

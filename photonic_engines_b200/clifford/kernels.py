@@ -56,6 +56,15 @@ def _i64(t, dev):
     return None if t is None else torch.as_tensor(t, dtype=torch.int64, device=dev).contiguous()
 
 
+def _seed_rows(seeds_t, seed_row_t):
+    """seed_row indexes the rows of seeds: checked on the host before a launch reads seeds with it."""
+    if seeds_t is None or seed_row_t is None or seed_row_t.numel() == 0:
+        return
+    lo, hi = int(seed_row_t.min()), int(seed_row_t.max())
+    if lo < 0 or hi >= seeds_t.shape[0]:
+        raise ValueError(f"seed_row: values in [0, {seeds_t.shape[0]}) expected (got {lo}..{hi})")
+
+
 def split_plan(heavy_streams: int, n: int, device, block_threads: int = 256, tpl: int = 2):
     """(k_split, nch) for a batch whose long chains number `heavy_streams`, or None when one CTA per stream
     already fills the GPU.  nch CTAs share every step k >= k_split of a stream; k_split is the first step
@@ -116,6 +125,10 @@ def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst
         seeds_t = seeds_t[None]
     if seeds_t is not None and seeds_t.shape[-1] != n_stride:
         seeds_t = torch.nn.functional.pad(seeds_t, (0, n_stride - seeds_t.shape[-1])).contiguous()
+    # converted tensors stay referenced until the launch is queued (temporaries freed inside the argument
+    # list would let the next conversion reuse their memory)
+    seed_row_t, rng_off_t, order_t = _i64(seed_row, dev), _i64(rng_off, dev), _i64(order, dev)
+    _seed_rows(seeds_t, seed_row_t)
     if out is not None:
         rows, occ, marg = out
     else:
@@ -125,7 +138,7 @@ def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst
     a = acol if acol.dtype == torch.float64 else torch.view_as_real(acol.contiguous())
     common = (N.PRECISIONS[precision], N.ptr(a), N.ptr(inst_off), N.ptr(inst_m), N.ptr(inst_n), int(inst_off.shape[0]),
               int(m_max), int(S), N.ptr(dp), N.ptr(nk_t), N.ptr(cols), int(n_stride), N.ptr(u_t), N.ptr(seeds_t),
-              N.ptr(_i64(seed_row, dev)), N.ptr(_i64(rng_off, dev)), N.ptr(_i64(order, dev)), N.ptr(rows), N.ptr(occ),
+              N.ptr(seed_row_t), N.ptr(rng_off_t), N.ptr(order_t), N.ptr(rows), N.ptr(occ),
               int(occ_stride), N.ptr(marg), int(m_max))
     if mode not in ("auto", "cta", "warp"):
         raise ValueError(f"unknown mode {mode!r}: 'auto', 'cta' or 'warp'")
@@ -151,6 +164,61 @@ def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst
         if st != 0:
             raise N.NativeError(f"pe_fock_chain: device-side index error at stream {det} (status {st})")
     return rows, occ, marg
+
+
+def chain_adaptive(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst_n: torch.Tensor, dp, cols,
+                   rows: torch.Tensor, n_prefix: int, *, m_max: int | None = None, avoid=None, uniforms=None,
+                   seeds=None, seed_row=None, rng_off=None, precision: str = "f64", block_threads: int = 0,
+                   tpl: int = 0, split=None, mode: str = "auto", check_status: bool = True):
+    """Adaptive chains (pe_fock_chain_adaptive): rows [S, n] int64 holds the forced prefix in its first
+    n_prefix columns and receives the rest; avoid: bool / uint8 [m_max] mask of avoided modes or None.
+    Every stream has n = cols.shape[1] photons.  Returns (rows, occ [S, m_max], alive [S] bool)."""
+    N.require_cuda(acol, "acol")
+    dev = acol.device
+    L = N.load()
+    if precision not in N.PRECISIONS:
+        raise ValueError(f"unknown precision {precision!r}: 'f64' or 'mixed'")
+    dp = _i64(dp, dev)
+    cols = _i64(cols, dev)
+    S, n = cols.shape
+    if n > N.PE_MAX_PHOTONS:
+        raise ValueError(f"at most {N.PE_MAX_PHOTONS} photons per stream (got {n})")
+    if m_max is None:
+        m_max = int(inst_m.max().item())
+    u_t = None if uniforms is None else torch.as_tensor(uniforms, dtype=torch.float64, device=dev).contiguous()
+    seeds_t = _i64(seeds, dev)
+    if u_t is None and seeds_t is None:
+        raise ValueError("either uniforms or seeds")
+    if seeds_t is not None and seeds_t.dim() == 1:
+        seeds_t = seeds_t[None]
+    seed_row_t, rng_off_t = _i64(seed_row, dev), _i64(rng_off, dev)
+    _seed_rows(seeds_t, seed_row_t)
+    av = None
+    if avoid is not None:
+        av = torch.as_tensor(avoid, device=dev).to(torch.uint8).contiguous()
+        if av.shape != (m_max,):
+            raise ValueError(f"avoid: a mask over the {m_max} output modes")
+    alive = torch.ones(S, dtype=torch.uint8, device=dev)
+    occ = torch.zeros(S, m_max, dtype=torch.int64, device=dev)
+    if mode not in ("auto", "cta", "warp"):
+        raise ValueError(f"unknown mode {mode!r}: 'auto', 'cta' or 'warp'")
+    warp = (mode == "warp") or (mode == "auto" and not split and use_warp_form(S, n, dev))
+    k_split, nch = (0, 0) if (warp or not split) else split
+    ws = torch.empty(int(L.pe_adaptive_workspace_bytes(S, nch)), dtype=torch.uint8, device=dev)
+    a = acol if acol.dtype == torch.float64 else torch.view_as_real(acol.contiguous())
+    rc = L.pe_fock_chain_adaptive(N.PRECISIONS[precision], N.ptr(a), N.ptr(inst_off), N.ptr(inst_m), N.ptr(inst_n),
+                                  int(inst_off.shape[0]), int(m_max), int(S), N.ptr(dp), N.ptr(cols), int(n),
+                                  N.ptr(u_t), N.ptr(seeds_t), N.ptr(seed_row_t), N.ptr(rng_off_t),
+                                  N.ptr(rows), int(n_prefix), N.ptr(av), N.ptr(alive), N.ptr(occ), int(m_max),
+                                  int(k_split), int(nch), N.ptr(ws), int(ws.numel()), int(block_threads),
+                                  int(tpl if (not warp or tpl in (1, 2)) else 0), 1 if warp else 0,
+                                  N.stream_handle(dev))
+    N.check(rc, "pe_fock_chain_adaptive")
+    if check_status:
+        st, det = N.read_status(ws)
+        if st != 0:
+            raise N.NativeError(f"pe_fock_chain_adaptive: device-side index error at stream {det} (status {st})")
+    return rows, occ, alive.bool()
 
 
 def laplace_cofactors_rows(A: torch.Tensor, rows: torch.Tensor, precision: str = "f64", block_threads: int = 0,

@@ -23,7 +23,8 @@ import torch
 
 from .. import _native as N
 from ..imperfections import partition, route_classical, spec
-from .kernels import chain, pack_instances, split_plan
+from .kernels import chain, chain_adaptive, pack_instances, split_plan
+from .prefix import prefix_order
 
 BACKENDS = ("b200", "triton", "cuda", "exq")
 ALGOS = ("auto", "2018", "2020", "input", "percof")
@@ -103,12 +104,33 @@ def fock_sample(U, in_modes, shots, generator=None, algo="auto", multi_min_k1=10
     marginals and CDF).  uniforms: optional float64 [S, n] per-step uniforms replacing the Philox draws
     (lossless only).  stats: receives "passes" = [(k, streams, seconds)] — all passes run in one launch, so
     every entry carries that launch's time — and "fused_seconds".
+    prefix (adaptive sampling, lossless only): the output modes the FIRST c photons of every chain are forced
+    onto — a list of c modes shared by all circuits, or an int tensor [B, c]; the column set of those c steps
+    is drawn from its posterior |per(A[prefix, T])|^2 (`prefix.prefix_columns_many`) and the chain runs steps
+    c + 1..n; the occupations include the prefix.  avoid: output modes no photon after the prefix may reach;
+    a stream is dropped as soon as one does, and only the survivors are returned ([S', m]; with keep_ids=True
+    the pair (occupations, surviving stream ids)).  Both as the reference's sampler.py:26-39, 391-460.
     """
     d = spec(indist)
-    if prefix is not None or (avoid is not None and len(avoid)):
+    if prefix is not None:
+        prefix = torch.as_tensor(prefix, dtype=torch.int64)
+        if prefix.dim() == 2 and prefix.shape[0] == 1 and U.dim() == 2:
+            prefix = prefix[0]
+        if prefix.numel() == 0:
+            prefix = None
+    avoid = [int(r) for r in avoid] if avoid is not None and len(avoid) else None
+    if prefix is not None or avoid is not None:
         if backend == "exq" or d is not None or not (loss is None or float(loss) >= 1.0):
             raise NotImplementedError("prefix / avoid: lossless, indistinguishable photons only")
-        raise NotImplementedError("prefix / avoid (adaptive sampling) are not available in this build")
+        nb = U.shape[0] if U.dim() == 3 else 1
+        if prefix is not None:
+            if prefix.dim() == 2 and prefix.shape[0] != nb:
+                raise ValueError(f"prefix [{prefix.shape[0]}, r]: one row per circuit ({nb})")
+            if (prefix.dim() > 2 or prefix.shape[-1] > len(in_modes) or bool((prefix < 0).any())
+                    or bool((prefix >= U.shape[-2]).any())):
+                raise ValueError(f"prefix: at most n = {len(in_modes)} output modes of the circuit")
+        if avoid is not None and any(not 0 <= r < U.shape[-2] for r in avoid):
+            raise ValueError(f"avoid {avoid}: output modes of the circuit")
     if backend not in BACKENDS:
         raise ValueError(f'unknown backend {backend!r} for a Fock input: "b200", "triton", "cuda" or "exq" '
                          f'("torch" exists on the emitter sampler only)')
@@ -147,6 +169,9 @@ def fock_sample(U, in_modes, shots, generator=None, algo="auto", multi_min_k1=10
         return (occ, torch.arange(S, device=dev, dtype=torch.int64)) if keep_ids else occ
     if uniforms is not None and not (lossless and d is None):
         raise NotImplementedError("uniforms=: lossless, indistinguishable photons only")
+    if prefix is not None or avoid is not None:
+        return _adaptive(U, in_modes, S, dp_all, generator, max_streams, prefix, avoid, keep_ids, stats,
+                         precision, uniforms, block_threads, tpl)
     plan = plan_chains(U, in_modes, S, dp_all, generator, loss, d, max_streams)
     acol, inst_off, inst_m, inst_n = pack_instances(U, in_modes)
     t0 = None
@@ -172,6 +197,56 @@ def fock_sample(U, in_modes, shots, generator=None, algo="auto", multi_min_k1=10
     if not direct:
         occ = assemble_occupations(plan, rows, m)
     return (occ, torch.arange(S, device=dev, dtype=torch.int64)) if keep_ids else occ
+
+
+def _adaptive(U, in_modes, S, dp_all, generator, max_streams, prefix, avoid, keep_ids, stats, precision, uniforms,
+              block_threads, tpl):
+    """fock_sample with a forced prefix and / or avoided modes (sampler.py:391-460 with prefix / avoid):
+    per pass chunk of max_streams streams the column order (prefix_order for a prefix, else argsort(rand))
+    and the step seeds, drawn as the reference draws them; then every chunk's chains in one call of the
+    adaptive chain kernel (one launch per step with avoid, the survivors renumbered on the device)."""
+    dev = U.device
+    n = len(in_modes)
+    m = U.shape[1]
+    c0 = 0 if prefix is None else prefix.shape[-1]
+    gdev = _draw_device(generator, dev)
+    A = U[:, :, list(in_modes)].to(torch.complex128)
+    sig, seeds, chunk, off = [], [], [], []
+    for ci, s0 in enumerate(range(0, S, max_streams)):
+        dpc = dp_all[s0:s0 + max_streams]
+        Sc = dpc.shape[0]
+        if c0:
+            sig.append(prefix_order(A, dpc, n, prefix.to(dev), generator).to(dev))
+        else:
+            sig.append(torch.argsort(torch.rand(Sc, n, generator=generator, device=gdev), dim=1).to(dev))
+        seeds.append(torch.randint(0, 2 ** 31 - 1, (n,), generator=generator, device=gdev).to(dev))
+        chunk.append(torch.full((Sc,), ci, dtype=torch.int64, device=dev))
+        off.append(torch.arange(Sc, dtype=torch.int64, device=dev))
+    rows = torch.zeros(S, n, dtype=torch.int64, device=dev)
+    if c0:
+        pre = prefix.to(dev)
+        rows[:, :c0] = pre[dp_all] if pre.dim() == 2 else pre
+    mask = None
+    if avoid is not None:
+        mask = torch.zeros(m, dtype=torch.uint8, device=dev)
+        mask[avoid] = 1
+    acol, inst_off, inst_m, inst_n = pack_instances(U, in_modes)
+    u = None if uniforms is None else torch.as_tensor(uniforms, dtype=torch.float64, device=dev)
+    t0 = None
+    if stats is not None:
+        torch.cuda.synchronize(dev)
+        t0 = _time.perf_counter()
+    _, occ, alive = chain_adaptive(acol, inst_off, inst_m, inst_n, dp_all, torch.cat(sig), rows, c0, m_max=m,
+                                   avoid=mask, uniforms=u, seeds=torch.stack(seeds), seed_row=torch.cat(chunk),
+                                   rng_off=torch.cat(off), precision=precision, block_threads=block_threads, tpl=tpl,
+                                   split=split_plan(S, n, dev, block_threads or 256, tpl or 2))
+    if stats is not None:
+        torch.cuda.synchronize(dev)
+        stats["fused_seconds"] = _time.perf_counter() - t0
+        stats.setdefault("passes", []).append((n, S, stats["fused_seconds"]))
+    if avoid is None:
+        return (occ, torch.arange(S, device=dev, dtype=torch.int64)) if keep_ids else occ
+    return (occ[alive], torch.nonzero(alive)[:, 0]) if keep_ids else occ[alive]
 
 
 @dataclass

@@ -87,6 +87,79 @@ __global__ void pipe_probe_kernel(T* out, T a, T b, int iters) {
     out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+
+// ---------------------------------------------------------------------------------------- adaptive
+// Survivors of an adaptive chain (one CTA of 1024 threads).  col < 0: initial state, every stream alive.
+// col >= 0: a live stream whose row rows[s][col] is an avoided mode is dropped.  Then nk[s] = n for the
+// survivors and 0 for dropped streams (the chain kernels skip those), and rng[s] = the rank of s among
+// the survivors of its pass chunk (chunk start s - off0[s]): the stream index the next step's draws use,
+// because the reference shrinks the batch after every drop and renumbers the survivors
+// (photonic_engines/clifford/sampler.py:436-446).  zero_dead: the occupation rows of dropped streams
+// are cleared (the last update).
+struct AvoidParams {
+    const int64_t* rows;
+    int n_stride;
+    int col;
+    const unsigned char* avoid;
+    int m_max;
+    unsigned char* alive;
+    int32_t* nk;
+    int64_t* rng;
+    int64_t* scan;
+    const int64_t* off0;
+    int64_t S;
+    int n;
+    int64_t* occ;
+    int occ_stride;
+    int zero_dead;
+    int* status;
+    long long* detail;
+};
+
+__global__ void __launch_bounds__(1024) avoid_update_kernel(AvoidParams a) {
+    __shared__ int64_t wsum[32];
+    const int tid = threadIdx.x, T = blockDim.x, lid = tid & 31, wid = tid >> 5;
+    for (int64_t s = tid; s < a.S; s += T) {
+        int live = a.col < 0 ? 1 : a.alive[s];
+        if (live && a.col >= 0) {
+            const int64_t r = a.rows[s * a.n_stride + a.col];
+            if (r < 0 || r >= a.m_max) { record_error(a.status, a.detail, s); live = 0; }
+            else if (a.avoid[r]) live = 0;
+        }
+        a.alive[s] = (unsigned char)live;
+        a.nk[s] = live ? a.n : 0;
+        if (!live && a.zero_dead && a.occ)
+            for (int rho = 0; rho < a.occ_stride; ++rho) a.occ[s * (int64_t)a.occ_stride + rho] = 0;
+    }
+    __syncthreads();
+    // exclusive scan of alive: a contiguous chunk per thread, warp scan, warps in order
+    const int64_t C = (a.S + T - 1) / T;
+    const int64_t lo = min((int64_t)tid * C, a.S), hi = min(lo + C, a.S);
+    int64_t loc = 0;
+    for (int64_t i = lo; i < hi; ++i) loc += a.alive[i];
+    int64_t x = loc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lid >= o) x += y;
+    }
+    if (lid == 31) wsum[wid] = x;
+    __syncthreads();
+    int64_t base = x - loc;
+    for (int w = 0; w < wid; ++w) base += wsum[w];
+    for (int64_t i = lo; i < hi; ++i) { a.scan[i] = base; base += a.alive[i]; }
+    __syncthreads();
+    for (int64_t s = tid; s < a.S; s += T) {
+        int64_t c = a.off0 ? s - a.off0[s] : 0;
+        if (c < 0 || c > s) { record_error(a.status, a.detail, s); c = s; }
+        a.rng[s] = a.scan[s] - a.scan[c];
+    }
+}
+
+static size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+static size_t split_bytes(int64_t S, int nch) {
+    return nch > 0 ? (size_t)S * nch * MAXN * sizeof(double2) + (size_t)S * sizeof(int) : 0;
+}
 }  // namespace pe
 
 using namespace pe;
@@ -140,15 +213,19 @@ static int launch_prepare(void* fn, int block, size_t smem, int* grid_per_sm) {
 
 // Checks, variant lookup and launches shared by the chain entry points.  k_split = 0: the whole chain in
 // the persistent kernel; k_split >= 2: steps 1..k_split-1 there, then every step k >= k_split spread over
-// nch CTAs per stream (split_partial) and drawn by one CTA per stream (split_draw).
+// nch CTAs per stream (split_partial) and drawn by one CTA per stream (split_draw).  Only the steps
+// k_first..k_last run (k_last 0: to the end of every chain); rows[:, :k_first - 1] are read from d_rows.
+// zero_status false keeps the status word of an earlier launch (the queue counter is always reset).
 static int chain_launch(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
                         const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
                         const int32_t* d_nk, const int64_t* d_cols, int n_stride, const double* d_uniforms,
                         const int64_t* d_seeds, const int64_t* d_seed_row, const int64_t* d_rng_off,
                         const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
                         int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
-                        int grid_ctas, int k_split, int nch, void* stream, bool warp_mode = false) {
+                        int grid_ctas, int k_split, int nch, void* stream, bool warp_mode = false,
+                        int k_first = 1, int k_last = 0, bool zero_status = true) {
     if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
+    if (k_first < 1 || k_first > n_stride + 1 || k_last < 0) return PE_ERR_ARG;
     if (S < 0 || G < 1 || m_max < 1 || n_stride < 1) return PE_ERR_ARG;
     if (!d_acol || !d_inst_off || !d_inst_m || !d_inst_n || !d_dp || !d_cols || !d_rows || !d_workspace) return PE_ERR_ARG;
     if (!d_uniforms && !d_seeds) return PE_ERR_ARG;
@@ -173,8 +250,10 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     if (cap <= 0) return PE_ERR_CUDA;
     if (smem > (size_t)cap) return PE_ERR_SIZE;
     cudaStream_t st = (cudaStream_t)stream;
-    if (cudaMemsetAsync(d_workspace, 0, WS_BYTES, st) != cudaSuccess) return PE_ERR_CUDA;
+    if (cudaMemsetAsync(d_workspace, 0, zero_status ? WS_BYTES : sizeof(unsigned long long), st) != cudaSuccess)
+        return PE_ERR_CUDA;
     if (S == 0) return PE_OK;
+    const int klast = (k_last > 0 && k_last < n_stride) ? k_last : n_stride;
     int per_sm = 0;
     int rc = launch_prepare(fn, block, smem, &per_sm);
     if (rc != PE_OK) return rc;
@@ -196,7 +275,8 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     p.detail = (long long*)((char*)d_workspace + 16);
     p.m_cap = m_max;
     p.tau = 1.0e-5;            // mixed guard band: 3x the largest measured CDF deviation (3.3e-6, n <= 28)
-    p.k_stop = split ? k_split - 1 : 0;
+    p.k_first = k_first;
+    p.k_stop = split ? (k_split - 1 < klast ? k_split - 1 : klast) : (k_last > 0 ? klast : 0);
     void* args[] = {&p};
     if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st) != cudaSuccess) return PE_ERR_CUDA;
     if (!split) return PE_OK;
@@ -220,7 +300,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     sp.partial = (double2*)((char*)d_workspace + WS_BYTES);
     sp.flag = (int*)((char*)d_workspace + WS_BYTES + part_bytes);
     void* sargs[] = {&sp};
-    for (int k = k_split; k <= n_stride; ++k) {
+    for (int k = (k_split > k_first ? k_split : k_first); k <= klast; ++k) {
         sp.k = k;
         for (int q = 0; q < npass; ++q) {
             sp.pass = q;
@@ -274,6 +354,67 @@ extern "C" int pe_fock_chain_split(int precision, const double* d_acol, const in
     return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, d_nk, d_cols, n_stride,
                         d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ, occ_stride, d_marg,
                         marg_stride, d_workspace, workspace_bytes, block_threads, tpl, 0, k_split, nch, stream);
+}
+
+extern "C" size_t pe_adaptive_workspace_bytes(int64_t S, int nch) {
+    const size_t s = (size_t)(S < 0 ? 0 : S);
+    return align16(WS_BYTES + split_bytes(S < 0 ? 0 : S, nch)) + align16(s * sizeof(int32_t)) + 2 * s * sizeof(int64_t);
+}
+
+extern "C" int pe_fock_chain_adaptive(int precision, const double* d_acol, const int64_t* d_inst_off,
+                                      const int32_t* d_inst_m, const int32_t* d_inst_n, int G, int m_max, int64_t S,
+                                      const int64_t* d_dp, const int64_t* d_cols, int n_stride,
+                                      const double* d_uniforms, const int64_t* d_seeds, const int64_t* d_seed_row,
+                                      const int64_t* d_rng_off, int64_t* d_rows, int n_prefix,
+                                      const uint8_t* d_avoid, uint8_t* d_alive, int64_t* d_occ, int occ_stride,
+                                      int k_split, int nch, void* d_workspace, size_t workspace_bytes,
+                                      int block_threads, int tpl, int mode, void* stream) {
+    if (n_prefix < 0 || n_prefix > n_stride || (mode != 0 && mode != 1)) return PE_ERR_ARG;
+    if (k_split < 0 || (k_split > 0 && (k_split < 2 || nch < 1))) return PE_ERR_ARG;
+    if (mode == 1 && k_split > 0) return PE_ERR_ARG;
+    if (d_avoid && !d_alive) return PE_ERR_ARG;
+    if (!d_rows || !d_workspace || S < 0) return PE_ERR_ARG;
+    const int ks = (k_split > 0 && k_split <= n_stride) ? k_split : 0;
+    const bool warp = mode == 1;
+    if (!d_avoid || n_prefix == n_stride) {
+        if (d_alive && S > 0 && cudaMemsetAsync(d_alive, 1, (size_t)S, (cudaStream_t)stream) != cudaSuccess)
+            return PE_ERR_CUDA;
+        return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, nullptr, d_cols,
+                            n_stride, d_uniforms, d_seeds, d_seed_row, d_rng_off, nullptr, d_rows, d_occ, occ_stride,
+                            nullptr, m_max, d_workspace, workspace_bytes, block_threads, tpl, 0, ks, nch, stream, warp,
+                            n_prefix + 1, 0, true);
+    }
+    if (workspace_bytes < pe_adaptive_workspace_bytes(S, ks ? nch : 0) || ((uintptr_t)d_workspace & 15u))
+        return PE_ERR_SIZE;
+    if (d_occ && occ_stride < m_max) return PE_ERR_ARG;
+    char* w = (char*)d_workspace;
+    const size_t o_nk = align16(WS_BYTES + split_bytes(S, ks ? nch : 0));
+    AvoidParams a;
+    a.rows = d_rows; a.n_stride = n_stride; a.avoid = d_avoid; a.m_max = m_max; a.alive = d_alive;
+    a.nk = (int32_t*)(w + o_nk);
+    a.rng = (int64_t*)(w + o_nk + align16((size_t)S * sizeof(int32_t)));
+    a.scan = a.rng + S;
+    a.off0 = d_rng_off; a.S = S; a.n = n_stride; a.occ = d_occ; a.occ_stride = occ_stride;
+    a.status = (int*)(w + 8);
+    a.detail = (long long*)(w + 16);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(d_workspace, 0, WS_BYTES, st) != cudaSuccess) return PE_ERR_CUDA;
+    if (S == 0) return PE_OK;
+    for (int k = n_prefix + 1; k <= n_stride; ++k) {
+        a.col = k == n_prefix + 1 ? -1 : k - 2;            // no check before the first free step
+        a.zero_dead = 0;
+        avoid_update_kernel<<<1, 1024, 0, st>>>(a);
+        if (cudaGetLastError() != cudaSuccess) return PE_ERR_CUDA;
+        const int rc = chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, a.nk,
+                                    d_cols, n_stride, d_uniforms, d_seeds, d_seed_row, a.rng, nullptr, d_rows,
+                                    k == n_stride ? d_occ : nullptr, occ_stride, nullptr, m_max, d_workspace,
+                                    workspace_bytes, block_threads, tpl, 0, ks, nch, stream, warp, k, k, false);
+        if (rc != PE_OK) return rc;
+    }
+    a.col = n_stride - 1;                                 // the last photon is checked too
+    a.zero_dead = 1;
+    avoid_update_kernel<<<1, 1024, 0, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
 }
 
 extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t* d_rows, int64_t S, int m, int K,

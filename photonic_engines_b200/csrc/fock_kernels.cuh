@@ -68,7 +68,9 @@ struct ChainParams {
     long long* detail;
     int m_cap;
     double tau;     // mixed form: relative guard band of the draw
-    int k_stop;     // run steps 1..min(nk, k_stop) only (0: all); later steps go to the split kernels
+    int k_stop;     // run steps up to min(nk, k_stop) only (0: all); later steps go to the split kernels
+    int k_first;    // first step to run (1: the whole chain); rows[s][0 .. k_first - 2] are given (a forced
+                    // prefix, or the steps of an earlier launch).  A stream with nk < k_first - 1 is skipped.
 };
 
 // Mixed form: FP32 inner blocks of at most this many terms, each starting from FP64 column sums.
@@ -805,11 +807,18 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
     int64_t off = 0;
     if (ok) { m = p.inst_m[g]; nin = p.inst_n[g]; off = p.inst_off[g]; }
     const int nk = p.nk ? p.nk[s] : p.n_stride;
+    const int kf = p.k_first;
+    if (nk < kf - 1) return;                                  // nothing to run (a dropped stream)
     ok = ok && nk >= 0 && nk <= p.n_stride && nk <= KPM && m >= 1 && m <= p.m_cap && m <= p.occ_stride;
     if (ok && tid < nk) {
         const int64_t c = p.cols[s * p.n_stride + tid];
         if (c < 0 || c >= nin) atomicOr(&sm.bad, 1);
         else sm.cols[tid] = (int)c;
+    }
+    if (ok && tid < kf - 1) {
+        const int64_t r = p.rows[s * p.n_stride + tid];
+        if (r < 0 || r >= m) atomicOr(&sm.bad, 1);
+        else sm.rows[tid] = (int)r;
     }
     if (!ok && tid == 0) sm.bad = 1;
     if (tid == 0) { sm.ngrp = 0; sm.lane0 = 0; sm.lane_mult = 1; }
@@ -818,9 +827,13 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
         if (tid == 0) record_error(p.status, p.detail, s);
         return;
     }
+    if (kf > 1) {
+        if (tid == 0) for (int i = 0; i < kf - 1; ++i) add_to_groups(sm, sm.rows[i]);
+        __syncthreads();
+    }
     const double2* A = p.acol + off;      // (rho, j) at A[j * m + rho]
     const int kend = (p.k_stop > 0 && p.k_stop < nk) ? p.k_stop : nk;
-    for (int k = 1; k <= kend; ++k) {
+    for (int k = kf; k <= kend; ++k) {
         const int K = k, K1 = k - 1;
         if (K1 == 0) {
             if (tid == 0) sm.P[0] = make_double2(1.0, 0.0);
@@ -849,7 +862,7 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
             draw_step(sm, wgt, A, 1, m, m, k, u, mrow, true);
         }
     }
-    for (int j = tid; j < kend; j += blockDim.x) p.rows[s * p.n_stride + j] = sm.rows[j];
+    for (int j = kf - 1 + tid; j < kend; j += blockDim.x) p.rows[s * p.n_stride + j] = sm.rows[j];
     if (p.occ && kend == nk) {
         for (int rho = tid; rho < p.occ_stride; rho += blockDim.x) {
             int c = 0;

@@ -240,22 +240,33 @@ __device__ void chain_warp(const ChainParams& p, WarpSmem& sm, int64_t s) {
     int64_t off = 0;
     if (ok) { m = p.inst_m[g]; nin = p.inst_n[g]; off = p.inst_off[g]; }
     const int nk = p.nk ? p.nk[s] : p.n_stride;
+    const int kf = p.k_first;
+    if (nk < kf - 1) return;                                  // nothing to run (a dropped stream)
     ok = ok && nk >= 0 && nk <= p.n_stride && nk <= KPW && m >= 1 && m <= p.m_cap && m <= p.occ_stride;
-    bool badcol = false;
+    bool bad = false;
     if (ok && lane < nk) {
         const int64_t c = p.cols[s * p.n_stride + lane];
-        if (c < 0 || c >= nin) badcol = true;
+        if (c < 0 || c >= nin) bad = true;
         else sm.cols[lane] = (int)c;
     }
-    if (!ok || __any_sync(0xffffffffu, badcol)) {
+    if (ok && lane < kf - 1) {
+        const int64_t r = p.rows[s * p.n_stride + lane];
+        if (r < 0 || r >= m) bad = true;
+        else sm.rows[lane] = (int)r;
+    }
+    if (!ok || __any_sync(0xffffffffu, bad)) {
         if (lane == 0) record_error(p.status, p.detail, s);
         __syncwarp();
         return;
     }
-    if (lane == 0) { sm.ngrp = 0; sm.lane0 = 0; sm.lane_mult = 1; }
+    if (lane == 0) {
+        sm.ngrp = 0; sm.lane0 = 0; sm.lane_mult = 1;
+        for (int i = 0; i < kf - 1; ++i) add_to_groups(sm, sm.rows[i]);
+    }
     __syncwarp();
     const double2* A = p.acol + off;
-    for (int k = 1; k <= nk; ++k) {
+    const int kend = (p.k_stop > 0 && p.k_stop < nk) ? p.k_stop : nk;
+    for (int k = kf; k <= kend; ++k) {
         const int K1 = k - 1;
         if (K1 == 0) {
             if (lane == 0) sm.P[0] = make_double2(1.0, 0.0);
@@ -286,8 +297,8 @@ __device__ void chain_warp(const ChainParams& p, WarpSmem& sm, int64_t s) {
         if (lane == 0) add_to_groups(sm, sm.rows[k - 1]);
         __syncwarp();
     }
-    for (int j = lane; j < nk; j += 32) p.rows[s * p.n_stride + j] = sm.rows[j];
-    if (p.occ) {
+    for (int j = kf - 1 + lane; j < kend; j += 32) p.rows[s * p.n_stride + j] = sm.rows[j];
+    if (p.occ && kend == nk) {
         for (int rho = lane; rho < p.occ_stride; rho += 32) {
             int c = 0;
             for (int j = 0; j < nk; ++j) c += (sm.rows[j] == rho) ? 1 : 0;

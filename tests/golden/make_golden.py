@@ -2,7 +2,7 @@
 
 Run in a container where the reference project is importable (it is NOT needed at test time):
 
-    python tests/golden/make_golden.py /path/to/photonic-engines
+    python tests/golden/make_golden.py /path/to/photonic-engines [philox steps chains adaptive]
 
 It imports the reference read-only and records, with CPU tensors and the Triton CPU interpreter:
 
@@ -14,6 +14,10 @@ It imports the reference read-only and records, with CPU tensors and the Triton 
                (cuda_rect.rect_cofactors_emul, real="long double", form="fock", cuda_rect.py:959-985),
                and step amplitudes (variants.step_amplitudes, variants.py:176-194) on the
                reference's own test steps (tests/clifford/test_variants.py:41-49).
+  adaptive.npz chains with a forced prefix and avoided modes: `_sample_streams(..., prefix=, avoid=)`
+               rows and surviving stream ids with the sigma / seeds the generator produced, and
+               `fock_sample(..., prefix=, avoid=, keep_ids=True)` occupations and ids (sampler.py:57-182,
+               367-460).
   chains.npz   whole chains drawn by the reference's sampler: `_sample_streams`
                (sampler.py:391-460) rows [S, n] in chain order, plus the sigma and per-step seeds
                the generator produced, and `fock_sample` occupations with loss / partial
@@ -183,14 +187,76 @@ def make_chains():
     np.savez_compressed(os.path.join(HERE, "chains.npz"), **out)
 
 
+# (name, m, in_modes, B circuits, shots, generator seed, U seed, prefix, avoid, max_streams)
+ADAPTIVE = [
+    ("pre_shared", 8, [0, 1, 2, 3, 4, 5], 1, 40, 21, 51, [3, 3], None, 1 << 18),
+    ("pre_avoid", 8, [0, 1, 2, 3, 4, 5], 1, 60, 22, 52, [2], [2, 5], 1 << 18),
+    ("avoid_only", 7, [0, 1, 2, 3], 1, 60, 23, 53, None, [0, 4], 1 << 18),
+    ("pre_batch", 6, [0, 1, 2, 3], 2, 30, 24, 54, [[1, 4], [2, 2]], [1, 2, 4], 1 << 18),
+    ("pre_chunks", 7, [0, 1, 2, 3, 4], 1, 50, 25, 55, [6], [6, 0], 16),
+    ("pre_full", 6, [0, 1, 2], 1, 12, 26, 56, [1, 1, 3], [0], 1 << 18),
+]
+
+
+def make_adaptive():
+    from photonic_engines.clifford import fock_sample
+    from photonic_engines.clifford import sampler as RS
+    from photonic_engines.clifford.cofactors_triton import cofactor_partials_multi
+    out = {}
+    for name, m, in_modes, Bn, shots, gseed, useed, prefix, avoid, max_streams in ADAPTIVE:
+        U = torch.stack([haar(m, useed + b) for b in range(Bn)])
+        n = len(in_modes)
+        S = Bn * shots
+        A2 = torch.view_as_real(U[:, :, in_modes].to(torch.complex128).contiguous())
+        dp = torch.arange(Bn, dtype=torch.int64).repeat_interleave(shots)
+        pre_t = None if prefix is None else torch.as_tensor(prefix, dtype=torch.int64)
+        mask = None
+        if avoid is not None:
+            mask = torch.zeros(m, dtype=torch.bool)
+            mask[avoid] = True
+        sig_l, seeds_l, rows_l, kept_l = [], [], [], []
+        gen = torch.Generator().manual_seed(gseed)
+        g2 = torch.Generator().manual_seed(gseed)
+        for c0 in range(0, S, max_streams):
+            dpc = dp[c0:c0 + max_streams].contiguous()
+            rows, kept = RS._sample_streams(A2, dpc, n, m, gen, "auto", 10, 1 << 16, 1 << 17, cofactor_partials_multi,
+                                            prefix=pre_t, avoid=mask)
+            if pre_t is not None:
+                sig = RS._prefix_order(A2, dpc, n, pre_t, g2)
+            else:
+                sig = torch.argsort(torch.rand(dpc.shape[0], n, generator=g2), dim=1)
+            seeds_l.append(torch.randint(0, 2 ** 31 - 1, (n,), generator=g2))
+            sig_l.append(sig)
+            full = torch.full((dpc.shape[0], n), -1, dtype=torch.int64)
+            ids = torch.arange(dpc.shape[0]) if kept is None else kept
+            full[ids] = rows
+            rows_l.append(full)
+            alive = torch.zeros(dpc.shape[0], dtype=torch.bool)
+            alive[ids] = True
+            kept_l.append(alive)
+        occ, oids = fock_sample(U if Bn > 1 else U[0], in_modes, shots, generator=torch.Generator().manual_seed(gseed),
+                                prefix=prefix, avoid=avoid, keep_ids=True, max_streams=max_streams)
+        out[f"{name}__U"] = U.numpy()
+        out[f"{name}__in_modes"] = np.array(in_modes)
+        out[f"{name}__meta"] = np.array([m, Bn, shots, gseed, useed, max_streams])
+        out[f"{name}__prefix"] = np.array(prefix if prefix is not None else [], dtype=np.int64)
+        out[f"{name}__avoid"] = np.array(avoid if avoid is not None else [], dtype=np.int64)
+        out[f"{name}__sigma"] = torch.cat(sig_l).numpy()
+        out[f"{name}__seeds"] = torch.stack(seeds_l).numpy()
+        out[f"{name}__rows"] = torch.cat(rows_l).numpy()          # -1 rows: a stream dropped by `avoid`
+        out[f"{name}__alive"] = torch.cat(kept_l).numpy()
+        out[f"{name}__occ"] = occ.numpy()
+        out[f"{name}__ids"] = oids.numpy()
+        print(name, "occ", tuple(occ.shape), flush=True)
+    np.savez_compressed(os.path.join(HERE, "adaptive.npz"), **out)
+
+
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PE_REFERENCE", "")
     if not ref or not os.path.isdir(ref):
         raise SystemExit("usage: make_golden.py /path/to/photonic-engines (the reference checkout)")
     sys.path.insert(0, ref)
-    make_philox()
-    print("philox done", flush=True)
-    make_steps()
-    print("steps done", flush=True)
-    make_chains()
-    print("chains done", flush=True)
+    parts = sys.argv[2:] or ["philox", "steps", "chains", "adaptive"]
+    for part in parts:
+        {"philox": make_philox, "steps": make_steps, "chains": make_chains, "adaptive": make_adaptive}[part]()
+        print(part, "done", flush=True)
