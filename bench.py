@@ -138,6 +138,7 @@ def run_b200(args):
     import torch.distributed as dist
 
     from photonic_engines_b200 import _native as NAT
+    from photonic_engines_b200 import replicas as REP
     from photonic_engines_b200.clifford import fock_sample
     from photonic_engines_b200.clifford.kernels import chain, pack_instances
     from photonic_engines_b200.clifford.work import chain_work
@@ -145,8 +146,7 @@ def run_b200(args):
     ws, rank, local = _dist()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if ws > 1:
-        dist.init_process_group("nccl", device_id=dev)
+    REP.init("nccl", device=dev)
     g = torch.Generator().manual_seed(USEED)
     z = torch.randn(M_MODES, M_MODES, generator=g, dtype=torch.float64) + 1j * torch.randn(
         M_MODES, M_MODES, generator=g, dtype=torch.float64)
@@ -157,7 +157,7 @@ def run_b200(args):
     in_modes = list(range(N_PHOT))
     acol, off, mm, nn = pack_instances(U, in_modes)
     dp = torch.zeros(SHOTS, dtype=torch.int64, device=dev)
-    gen = torch.Generator(device=dev).manual_seed(1000 + rank)
+    gen = torch.Generator(device=dev).manual_seed(REP.replica_seed(1000, rank))
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     rows_buf = torch.empty(SHOTS, N_PHOT, dtype=torch.int64, device=dev)
     occ_buf = torch.empty(SHOTS, M_MODES, dtype=torch.int64, device=dev)
@@ -174,12 +174,7 @@ def run_b200(args):
         if ws > 1:
             dist.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = REP.max_over_ranks
 
     def timed(precision, steps, warmup):
         for _ in range(warmup):
@@ -231,7 +226,7 @@ def run_b200(args):
     # end to end through the public API: U from pinned host memory, occupations back to the host
     U_pin = U_host.pin_memory()
     out_pin = torch.empty(SHOTS, M_MODES, dtype=torch.int64).pin_memory()
-    gen_e2e = torch.Generator(device=dev).manual_seed(7 + rank)
+    gen_e2e = torch.Generator(device=dev).manual_seed(REP.replica_seed(7, rank))
 
     def e2e_step():
         Ud = U_pin.to(dev, non_blocking=True)
