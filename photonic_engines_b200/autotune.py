@@ -15,7 +15,7 @@ import torch
 WARP_CANDIDATES = [(1, 256), (2, 256)]          # the warp form: threads per lane; the CTA is 8 warps
 CANDIDATES = {8: [(1, 128), (1, 256), (2, 128), (2, 256)],
               16: [(1, 128), (2, 128), (2, 256), (4, 256)],
-              20: [(2, 128), (2, 256), (4, 128), (4, 256)],
+              20: [(1, 128), (2, 128), (2, 256), (4, 128), (4, 256)],
               24: [(2, 128), (2, 256), (4, 128), (4, 256)],
               28: [(2, 256), (4, 128), (4, 256)],
               32: [(2, 256), (4, 128), (4, 256)]}

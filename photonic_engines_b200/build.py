@@ -24,10 +24,18 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.
          *os.environ.get("PE_NVCC_FLAGS", "").split()]
 
 # (mixed, threads per lane, largest tier) of every compiled chain/cofactor kernel pair
-VARIANTS = [(mx, tpl, kpm) for mx in (0, 1) for tpl, kpms in ((1, (8, 16)), (2, (8, 16, 20, 24, 28, 32)),
+VARIANTS = [(mx, tpl, kpm) for mx in (0, 1) for tpl, kpms in ((1, (8, 16, 20)), (2, (8, 16, 20, 24, 28, 32)),
                                                               (4, (8, 16, 20, 24, 28, 32))) for kpm in kpms]
 if os.environ.get("PE_VARIANTS"):          # a subset "m,t,k;m,t,k" (experiments: smaller, faster builds)
     VARIANTS = [tuple(int(x) for x in v.split(",")) for v in os.environ["PE_VARIANTS"].split(";")]
+
+
+def variant_flags(mx: int, tpl: int, kpm: int) -> list[str]:
+    """One-thread lanes of 16 and 20 columns hold up to 80 complex values per thread: they are compiled
+    for 128-thread CTAs, two per SM, so that every thread may use 255 registers."""
+    if tpl == 1 and kpm >= 16:
+        return ["-DPE_MAXT=128", "-DPE_MINB=2"]
+    return []
 
 
 def _sources():
@@ -58,7 +66,8 @@ def build(jobs: int | None = None, verbose: bool = False, ptxas_info: bool = Fal
         obj = os.path.join(OBJ, f"fock_m{mx}_t{tpl}_k{kpm}.o")
         if _stale(obj, deps):
             tasks.append([NVCC, *ARCH, *FLAGS, *(["-Xptxas", "-v"] if ptxas_info else []), f"-DPE_MIXED={mx}",
-                          f"-DPE_TPL={tpl}", f"-DPE_KPM={kpm}", "-c", os.path.join(CSRC, "fock_inst.cu"), "-o", obj])
+                          f"-DPE_TPL={tpl}", f"-DPE_KPM={kpm}", *variant_flags(mx, tpl, kpm), "-c",
+                          os.path.join(CSRC, "fock_inst.cu"), "-o", obj])
     extra = []
     for name in ("fock_api", "fock_batch"):
         obj = os.path.join(OBJ, f"{name}.o")

@@ -19,7 +19,7 @@ import torch
 
 from .. import _native as N
 from .. import autotune
-from .kernels import pack_ragged, split_plan, use_warp_form
+from .kernels import default_tpl, pack_ragged, split_plan, use_warp_form
 
 
 def _per_instance(v, G, default):
@@ -94,7 +94,8 @@ class BatchedSampler:
         self.occ = torch.zeros(S, self.m_max, dtype=torch.int64, device=dev)
         self.status = torch.zeros(2, dtype=torch.int32, device=dev)
         self.warp = use_warp_form(self.S, self.n_stride, dev)           # short chains: one warp per stream
-        self.split = None if self.warp else split_plan(self.S, self.n_stride, dev, 256, 2)   # few long chains
+        self.split = None if self.warp else split_plan(self.S, self.n_stride, dev, 0,           # few long chains
+                                                        default_tpl(self.n_stride, precision))
         if self.split:
             self.ws = torch.empty(int(N.load().pe_chain_split_workspace_bytes(C, self.split[1])), dtype=torch.uint8,
                                   device=dev)

@@ -65,15 +65,27 @@ def _seed_rows(seeds_t, seed_row_t):
         raise ValueError(f"seed_row: values in [0, {seeds_t.shape[0]}) expected (got {lo}..{hi})")
 
 
-def split_plan(heavy_streams: int, n: int, device, block_threads: int = 256, tpl: int = 2):
+DEFAULT_BLOCK = 128          # the library's CTA size when the caller passes 0 (pe_fock_chain)
+
+
+def default_tpl(n: int, precision: str) -> int:
+    """Threads per Gray lane the library picks when the caller passes 0 (fock_api.cu default_tpl)."""
+    kpm = next((k for k in (8, 16, 20, 24, 28, 32) if n <= k), 32)
+    if kpm <= 8 or (precision == "f64" and kpm <= 20):
+        return 1
+    return 2 if kpm <= 24 else 4
+
+
+def split_plan(heavy_streams: int, n: int, device, block_threads: int = 0, tpl: int = 2):
     """(k_split, nch) for a batch whose long chains number `heavy_streams`, or None when one CTA per stream
     already fills the GPU.  nch CTAs share every step k >= k_split of a stream; k_split is the first step
     with enough Gray terms (2^(k-2)) for every CTA to run several lanes."""
-    slots = 2 * torch.cuda.get_device_properties(device).multi_processor_count
+    block = block_threads or DEFAULT_BLOCK
+    slots = torch.cuda.get_device_properties(device).multi_processor_count * max(1, 512 // block)
     if heavy_streams >= slots or n < 8:
         return None
     nch = min(64, -(-2 * slots // max(heavy_streams, 1)))
-    lanes = (block_threads or 256) // max(tpl, 1)
+    lanes = block // max(tpl, 1)
     k = 2
     while k <= n and (1 << (k - 2)) < 4 * nch * lanes:
         k += 1

@@ -37,7 +37,9 @@ void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cof
     g_chain[mixed][ti][ki] = chain_kernel;
     g_cof[mixed][ti][ki] = cofactor_kernel;
     g_split_partial[mixed][ti][ki] = split_partial;
-    g_split_draw[mixed][ki] = split_draw;
+    // the draw kernel does not depend on the lane width; keep one compiled for 256-thread CTAs (the
+    // one-thread-lane variants of 16 and 20 columns are compiled for 128)
+    if (!g_split_draw[mixed][ki] || tpl != 1) g_split_draw[mixed][ki] = split_draw;
 }
 void* find_split_partial_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
@@ -61,7 +63,21 @@ void* find_cofactor_kernel(int mixed, int tpl, int kpm) {
     return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_cof[mixed][ti][ki];
 }
 
-static int default_tpl(int kpm) { return kpm <= 8 ? 1 : (kpm <= 24 ? 2 : 4); }
+// Threads per Gray lane when the caller passes 0: one-thread lanes (no exchange of partial products)
+// wherever their registers fit — up to 20 columns in FP64, whose variants run 128-thread CTAs with 255
+// registers — two-thread lanes up to 24 columns, four beyond.
+static int default_tpl(int kpm, int precision) {
+    if (kpm <= 8) return 1;
+    if (precision == PE_PRECISION_F64 && kpm <= 20) return 1;
+    return kpm <= 24 ? 2 : 4;
+}
+
+// Largest CTA a compiled kernel accepts (its launch bounds).
+static int max_block(void* fn) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, fn) != cudaSuccess) return 0;
+    return a.maxThreadsPerBlock;
+}
 
 static int max_smem_optin() {
     int dev = 0, v = 0;
@@ -239,12 +255,19 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     const int kpm = kpm_for(n_stride);
     if (kpm < 0) return PE_ERR_SIZE;
     if (warp_mode && (kpm > WMAXN || split)) return PE_ERR_SIZE;
-    if (tpl == 0) tpl = warp_mode ? (kpm <= 8 ? 1 : 2) : default_tpl(kpm);
+    if (tpl == 0) {
+        tpl = warp_mode ? (kpm <= 8 ? 1 : 2) : default_tpl(kpm, precision);
+        if (!warp_mode && !find_chain_kernel(precision, tpl, kpm)) tpl = kpm <= 24 ? 2 : 4;
+    }
     if (tpl_index(tpl) < 0) return PE_ERR_ARG;
     void* fn = warp_mode ? find_warp_kernel(precision, tpl, kpm) : find_chain_kernel(precision, tpl, kpm);
     if (!fn) return PE_ERR_SIZE;
-    const int block = warp_mode ? 32 * WARPS : (block_threads ? block_threads : 256);
-    if (block < 32 || block > 256 || (block & 31)) return PE_ERR_ARG;
+    const int bmax = max_block(fn);
+    if (bmax < 32) return PE_ERR_CUDA;
+    // default CTA: 128 threads (as many warps per SM as 256-thread CTAs, twice the CTAs to overlap the
+    // per-step serial phases of one stream with the sweeps of others)
+    const int block = warp_mode ? 32 * WARPS : (block_threads ? block_threads : (bmax < 128 ? bmax : 128));
+    if (block < 32 || block > 256 || block > bmax || (block & 31)) return PE_ERR_ARG;
     const size_t smem = warp_mode ? warp_smem_bytes() : smem_fixed_bytes() + (size_t)m_max * sizeof(double);
     const int cap = max_smem_optin();
     if (cap <= 0) return PE_ERR_CUDA;
@@ -426,7 +449,7 @@ extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t
     if (workspace_bytes < WS_BYTES || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
     const int kpm = kpm_for(K);
     if (kpm < 0) return PE_ERR_SIZE;
-    if (tpl == 0) tpl = default_tpl(kpm);
+    if (tpl == 0) tpl = kpm <= 8 ? 1 : (kpm <= 24 ? 2 : 4);
     if (tpl_index(tpl) < 0) return PE_ERR_ARG;
     void* fn = find_cofactor_kernel(precision, tpl, kpm);
     if (!fn) return PE_ERR_SIZE;

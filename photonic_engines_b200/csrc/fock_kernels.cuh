@@ -36,8 +36,11 @@
 #ifndef PE_SPLIT
 #define PE_SPLIT 1          // FP64: split a thread's product chain in two interleaved halves (1-/2-thread lanes)
 #endif
+#ifndef PE_MAXT
+#define PE_MAXT 256         // largest CTA the chain kernels are compiled for
+#endif
 #ifndef PE_MINB
-#define PE_MINB 2           // resident 256-thread CTAs per SM the register allocation must allow
+#define PE_MINB 2           // resident PE_MAXT-thread CTAs per SM the register allocation must allow
 #endif
 
 namespace pe {
@@ -258,12 +261,6 @@ static __device__ __forceinline__ int middle_digit(const Plan& pl, int pm, int q
 }
 
 // ---------------------------------------------------------------------------------------- sweep
-template <int TPL>
-__device__ __forceinline__ unsigned group_mask() {
-    if constexpr (TPL == 1) return 0u;
-    else return ((1u << TPL) - 1u) << ((threadIdx.x & 31) & ~(TPL - 1));
-}
-
 // Product of the other three threads' totals of a 4-thread lane: all three are gathered with
 // independent shuffles (one shuffle latency), then multiplied.
 template <int TPL, typename R>
@@ -610,15 +607,20 @@ __device__ void sweep_f64(Smem& sm) {
     const Plan& pl = sm.plan;
     const int tid = threadIdx.x;
     const int lanes = blockDim.x / TPL, lane = tid / TPL, h = tid % TPL, c0 = h * KH;
-    const unsigned gmask = group_mask<TPL>();
+    const int wl0 = (tid & ~31) / TPL;                     // first lane of this warp
+    const unsigned gmask = 0xffffffffu;                    // the warp walks its lanes in lockstep
     const int K = pl.K, Lin = pl.Lin, Lmid = pl.Lmid, nin = pl.nin;
     const int64_t H = pl.H;
     double ar[KH], ai[KH];
 #pragma unroll
     for (int j = 0; j < KH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
-    for (int64_t hl = sm.lane0 + lane; hl < H; hl += (int64_t)lanes * sm.lane_mult) {
+    for (int64_t hw = sm.lane0 + wl0; hw < H; hw += (int64_t)lanes * sm.lane_mult) {
         double sr[KH], si[KH], wh;
+        int64_t hl = hw + (lane - wl0);
+        const bool live = hl < H;                          // a lane past the end repeats lane H - 1 at weight 0
+        if (!live) hl = H - 1;
         const uint64_t hpack = lane_digits(pl, hl, &wh);
+        if (!live) wh = 0.0;
         lane_sums<KH>(sm, c0, false, 0, hl, hpack, sr, si);
 #pragma unroll
         for (int j = 0; j < KH; ++j) if (c0 + j >= K) { sr[j] = 1.0; si[j] = 0.0; }
@@ -646,15 +648,20 @@ __device__ void sweep_mixed(Smem& sm) {
     const Plan& pl = sm.plan;
     const int tid = threadIdx.x;
     const int lanes = blockDim.x / TPL, lane = tid / TPL, h = tid % TPL, c0 = h * KH;
-    const unsigned gmask = group_mask<TPL>();
+    const int wl0 = (tid & ~31) / TPL;
+    const unsigned gmask = 0xffffffffu;
     const int K = pl.K, Lin = pl.Lin, Lmid = pl.Lmid;
     const int64_t H = pl.H;
     double ar[KH], ai[KH];
 #pragma unroll
     for (int j = 0; j < KH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
-    for (int64_t hl = sm.lane0 + lane; hl < H; hl += (int64_t)lanes * sm.lane_mult) {
+    for (int64_t hw = sm.lane0 + wl0; hw < H; hw += (int64_t)lanes * sm.lane_mult) {
         double wh;
+        int64_t hl = hw + (lane - wl0);
+        const bool live = hl < H;
+        if (!live) hl = H - 1;
         const uint64_t hpack = lane_digits(pl, hl, &wh);
+        if (!live) wh = 0.0;
         for (int pm = 0; pm < Lmid; ++pm) {
             const bool fwd = !(pm & 1);
             float sr[KH], si[KH];
@@ -875,7 +882,7 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
 __host__ __device__ constexpr size_t smem_fixed_bytes() { return (sizeof(Smem) + 15) & ~(size_t)15; }
 
 template <int TPL, int KPM, bool MIXED>
-__global__ void __launch_bounds__(256, PE_MINB) fock_chain_kernel(ChainParams p) {
+__global__ void __launch_bounds__(PE_MAXT, PE_MINB) fock_chain_kernel(ChainParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
     double* wgt = reinterpret_cast<double*>(smem_raw + smem_fixed_bytes());
@@ -949,7 +956,7 @@ static __device__ bool load_state(const ChainParams& p, Smem& sm, int64_t s, int
 }
 
 template <int TPL, int KPM, bool MIXED>
-__global__ void __launch_bounds__(256, PE_MINB) split_partial_kernel(SplitParams sp) {
+__global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_partial_kernel(SplitParams sp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
     const ChainParams& p = sp.c;
@@ -971,7 +978,7 @@ __global__ void __launch_bounds__(256, PE_MINB) split_partial_kernel(SplitParams
 }
 
 template <int KPM, bool MIXED>
-__global__ void __launch_bounds__(256, PE_MINB) split_draw_kernel(SplitParams sp) {
+__global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_draw_kernel(SplitParams sp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
     double* wgt = reinterpret_cast<double*>(smem_raw + ((sizeof(Smem) + 15) & ~(size_t)15));

@@ -87,15 +87,19 @@ __device__ void sweep_warp_f64(WarpSmem& sm) {
     const Plan& pl = sm.plan;
     const int lane_id = threadIdx.x & 31;
     const int lanes = 32 / TPL, lane = lane_id / TPL, h = lane_id % TPL, c0 = h * KH;
-    const unsigned gmask = group_mask<TPL>();
+    const unsigned gmask = 0xffffffffu;                    // the warp walks its lanes in lockstep
     const int K = pl.K, Lin = pl.Lin, Lmid = pl.Lmid, nin = pl.nin;
     const int64_t H = pl.H;
     double ar[KH], ai[KH];
 #pragma unroll
     for (int j = 0; j < KH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
-    for (int64_t hl = lane; hl < H; hl += lanes) {
+    for (int64_t hw = 0; hw < H; hw += lanes) {
         double sr[KH], si[KH], wh;
+        int64_t hl = hw + lane;
+        const bool live = hl < H;                          // a lane past the end repeats lane H - 1 at weight 0
+        if (!live) hl = H - 1;
         const uint64_t hpack = lane_digits(pl, hl, &wh);
+        if (!live) wh = 0.0;
         lane_sums<KH>(sm, c0, false, 0, hl, hpack, sr, si);
 #pragma unroll
         for (int j = 0; j < KH; ++j) if (c0 + j >= K) { sr[j] = 1.0; si[j] = 0.0; }
@@ -121,15 +125,19 @@ __device__ void sweep_warp_mixed(WarpSmem& sm) {
     const Plan& pl = sm.plan;
     const int lane_id = threadIdx.x & 31;
     const int lanes = 32 / TPL, lane = lane_id / TPL, h = lane_id % TPL, c0 = h * KH;
-    const unsigned gmask = group_mask<TPL>();
+    const unsigned gmask = 0xffffffffu;
     const int K = pl.K, Lin = pl.Lin, Lmid = pl.Lmid;
     const int64_t H = pl.H;
     double ar[KH], ai[KH];
 #pragma unroll
     for (int j = 0; j < KH; ++j) { ar[j] = 0.0; ai[j] = 0.0; }
-    for (int64_t hl = lane; hl < H; hl += lanes) {
+    for (int64_t hw = 0; hw < H; hw += lanes) {
         double wh;
+        int64_t hl = hw + lane;
+        const bool live = hl < H;
+        if (!live) hl = H - 1;
         const uint64_t hpack = lane_digits(pl, hl, &wh);
+        if (!live) wh = 0.0;
         for (int pm = 0; pm < Lmid; ++pm) {
             const bool fwd = !(pm & 1);
             float sr[KH], si[KH];
