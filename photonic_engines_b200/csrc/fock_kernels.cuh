@@ -36,6 +36,9 @@
 #ifndef PE_SPLIT
 #define PE_SPLIT 1          // FP64: split a thread's product chain in two interleaved halves (1-/2-thread lanes)
 #endif
+#ifndef PE_PAIR32
+#define PE_PAIR32 1         // mixed form, 1- and 2-thread lanes: paired FP32 instructions (FFMA2 / FMUL2)
+#endif
 #ifndef PE_MAXT
 #define PE_MAXT 256         // largest CTA the chain kernels are compiled for
 #endif
@@ -224,8 +227,12 @@ static __device__ __forceinline__ unsigned char gray_entry(const Plan& pl, int d
     return (unsigned char)(qstar | (dir > 0 ? 0x80 : 0));
 }
 
-// All threads.  Element (rho, j) of the instance is A[rho * rs + j * cs].
-static __device__ void prepare_step(Smem& sm, const double2* __restrict__ A, int64_t rs, int64_t cs, bool mixed) {
+// All threads.  Element (rho, j) of the instance is A[rho * rs + j * cs].  kh > 0 (mixed form with
+// paired FP32 sweeps, kh columns per thread): row kd of B32 is written as float4 slots
+// q = h * kh/2 + c holding (re b_j1, re b_j2, im b_j1, im b_j2) of 2b, j1 = h * kh + c, j2 = j1 + kh/2 —
+// the two columns whose product chains one paired instruction advances together.
+static __device__ void prepare_step(Smem& sm, const double2* __restrict__ A, int64_t rs, int64_t cs, bool mixed,
+                                    int kh = 0) {
     const Plan& pl = sm.plan;
     const int tid = threadIdx.x, T = blockDim.x;
     for (int idx = tid; idx < pl.D * MAXN; idx += T) {
@@ -233,7 +240,19 @@ static __device__ void prepare_step(Smem& sm, const double2* __restrict__ A, int
         double2 b = make_double2(0.0, 0.0);
         if (j < pl.K) b = A[(int64_t)pl.drow[kd] * rs + (int64_t)sm.cols[j] * cs];
         sm.B[kd][j] = b;
-        if (mixed) sm.B32[kd][j] = make_float2((float)(2.0 * b.x), (float)(2.0 * b.y));
+        if (mixed && kh == 0) sm.B32[kd][j] = make_float2((float)(2.0 * b.x), (float)(2.0 * b.y));
+    }
+    if (mixed && kh > 0) {
+        __syncthreads();
+        const int ka = kh / 2;
+        for (int idx = tid; idx < pl.D * (MAXN / 2); idx += T) {
+            const int kd = idx / (MAXN / 2), q = idx % (MAXN / 2);
+            const int j1 = (q / ka) * kh + q % ka, j2 = j1 + ka;
+            const double2 b1 = j1 < pl.K ? sm.B[kd][j1] : make_double2(0.0, 0.0);
+            const double2 b2 = j2 < pl.K ? sm.B[kd][j2] : make_double2(0.0, 0.0);
+            reinterpret_cast<float4*>(&sm.B32[kd][0])[q] =
+                make_float4((float)(2.0 * b1.x), (float)(2.0 * b2.x), (float)(2.0 * b1.y), (float)(2.0 * b2.y));
+        }
     }
     for (int t = tid; t < pl.Lin; t += T) {
         double w;
@@ -516,6 +535,90 @@ __device__ __forceinline__ void inner_block(R (&sr)[KH], R (&si)[KH], R (&ar)[KH
     }
 }
 
+// ---------------------------------------------------------------------------------------- paired FP32
+// The mixed form's term on Blackwell's paired FP32 instructions (FFMA2 / FMUL2: two lanes of a float2 in
+// one issue slot).  A thread's KH columns are two halves [0, KA) and [KA, KH) whose product chains run
+// side by side in the two halves of every float2: sr[c] = (re s_c, re s_{KA+c}), si[c] likewise, and the
+// same for the prefix products and the accumulators.  Arithmetic as term_split (FP32).
+static __device__ __forceinline__ float2 f2neg(float2 a) { return make_float2(-a.x, -a.y); }
+
+template <int KH, int TPL>
+__device__ __forceinline__ void term_pair(float2 (&sr)[KH / 2], float2 (&si)[KH / 2], float2 (&ar)[KH / 2],
+                                          float2 (&ai)[KH / 2], const float4* brow, float f, float w, int h,
+                                          unsigned gmask) {
+    constexpr int KA = KH / 2;
+    if (brow) {
+        const float2 ff = make_float2(f, f);
+#pragma unroll
+        for (int c = 0; c < KA; ++c) {
+            const float4 b = brow[c];
+            sr[c] = __ffma2_rn(ff, make_float2(b.x, b.y), sr[c]);
+            si[c] = __ffma2_rn(ff, make_float2(b.z, b.w), si[c]);
+        }
+    }
+    const float2 w0 = make_float2((h == 0) ? w : 1.0f, 1.0f);
+    float2 pr[KA], pi[KA];
+    pr[0] = w0;
+    pi[0] = make_float2(0.0f, 0.0f);
+    float2 xr = __fmul2_rn(w0, sr[0]), xi = __fmul2_rn(w0, si[0]);
+#pragma unroll
+    for (int c = 1; c < KA; ++c) {
+        pr[c] = xr;
+        pi[c] = xi;
+        const float2 nr = __ffma2_rn(xr, sr[c], f2neg(__fmul2_rn(xi, si[c])));
+        xi = __ffma2_rn(xr, si[c], __fmul2_rn(xi, sr[c]));
+        xr = nr;
+    }
+    float2 yr, yi;                        // suffix starts: (other half's total) x (the partner's total)
+    if constexpr (TPL == 1) {
+        yr = make_float2(xr.y, xr.x);
+        yi = make_float2(xi.y, xi.x);
+    } else {
+        const float tr = fmaf(xr.x, xr.y, -(xi.x * xi.y)), ti = fmaf(xr.x, xi.y, xi.x * xr.y);
+        const float Yr = __shfl_xor_sync(gmask, tr, 1), Yi = __shfl_xor_sync(gmask, ti, 1);
+        const float2 br = make_float2(xr.y, xr.x), bi = make_float2(xi.y, xi.x);
+        const float2 YR = make_float2(Yr, Yr), YI = make_float2(Yi, Yi);
+        yr = __ffma2_rn(br, YR, f2neg(__fmul2_rn(bi, YI)));
+        yi = __ffma2_rn(br, YI, __fmul2_rn(bi, YR));
+    }
+#pragma unroll
+    for (int c = KA - 1; c >= 1; --c) {
+        ar[c] = __ffma2_rn(pr[c], yr, ar[c]);
+        ar[c] = __ffma2_rn(f2neg(pi[c]), yi, ar[c]);
+        ai[c] = __ffma2_rn(pr[c], yi, ai[c]);
+        ai[c] = __ffma2_rn(pi[c], yr, ai[c]);
+        const float2 nr = __ffma2_rn(yr, sr[c], f2neg(__fmul2_rn(yi, si[c])));
+        yi = __ffma2_rn(yr, si[c], __fmul2_rn(yi, sr[c]));
+        yr = nr;
+    }
+    ar[0] = __ffma2_rn(pr[0], yr, ar[0]);
+    ai[0] = __ffma2_rn(pr[0], yi, ai[0]);
+}
+
+// One paired inner block, forward or backward (B32 pre-doubled: the update magnitude is 1).
+template <int KH, int TPL, class SM>
+__device__ __forceinline__ void inner_block_pair(float2 (&sr)[KH / 2], float2 (&si)[KH / 2], float2 (&ar)[KH / 2],
+                                                 float2 (&ai)[KH / 2], const SM& sm, bool fwd, int Lin, int h,
+                                                 unsigned gmask) {
+    constexpr int KA = KH / 2;
+    const int q0 = h * KA;
+    if (fwd) {
+        term_pair<KH, TPL>(sr, si, ar, ai, nullptr, 0.0f, sm.tab_w32[0], h, gmask);
+        for (int t = 1; t < Lin; ++t) {
+            const unsigned e = sm.tab_f[t];
+            term_pair<KH, TPL>(sr, si, ar, ai, reinterpret_cast<const float4*>(&sm.B32[e & 63u][0]) + q0,
+                               (e & 0x80u) ? -1.0f : 1.0f, sm.tab_w32[t], h, gmask);
+        }
+    } else {
+        term_pair<KH, TPL>(sr, si, ar, ai, nullptr, 0.0f, sm.tab_w32[Lin - 1], h, gmask);
+        for (int t = Lin - 2; t >= 0; --t) {
+            const unsigned e = sm.tab_f[t + 1];
+            term_pair<KH, TPL>(sr, si, ar, ai, reinterpret_cast<const float4*>(&sm.B32[e & 63u][0]) + q0,
+                               (e & 0x80u) ? 1.0f : -1.0f, sm.tab_w32[t], h, gmask);
+        }
+    }
+}
+
 // Deterministic reduction of the per-thread accumulators over the lanes of the CTA -> sm.P.
 template <int KH, int TPL>
 __device__ __forceinline__ void reduce_to_P(double (&ar)[KH], double (&ai)[KH], Smem& sm, int c0) {
@@ -675,14 +778,37 @@ __device__ void sweep_mixed(Smem& sm) {
                     si[j] = pad ? 0.0f : (float)xi[j];
                 }
             }
-            float a32r[KH], a32i[KH];
-#pragma unroll
-            for (int j = 0; j < KH; ++j) { a32r[j] = 0.0f; a32i[j] = 0.0f; }
-            inner_block<KH, TPL, PE_UNROLL, float, float2, float>(sr, si, a32r, a32i, sm, sm.B32, sm.tab_w32, 1.0f, 1.0f,
-                                                                 fwd, Lin, c0, h, gmask);
             const double wmh = wh * sm.tab_wm[pm];
+            if constexpr (PE_PAIR32 && TPL <= 2 && KH % 2 == 0) {
+                constexpr int KA = KH / 2;
+                float2 s2r[KA], s2i[KA], a2r[KA], a2i[KA];
 #pragma unroll
-            for (int j = 0; j < KH; ++j) { ar[j] = fma(wmh, (double)a32r[j], ar[j]); ai[j] = fma(wmh, (double)a32i[j], ai[j]); }
+                for (int c = 0; c < KA; ++c) {
+                    s2r[c] = make_float2(sr[c], sr[KA + c]);
+                    s2i[c] = make_float2(si[c], si[KA + c]);
+                    a2r[c] = make_float2(0.0f, 0.0f);
+                    a2i[c] = make_float2(0.0f, 0.0f);
+                }
+                inner_block_pair<KH, TPL>(s2r, s2i, a2r, a2i, sm, fwd, Lin, h, gmask);
+#pragma unroll
+                for (int c = 0; c < KA; ++c) {
+                    ar[c] = fma(wmh, (double)a2r[c].x, ar[c]);
+                    ai[c] = fma(wmh, (double)a2i[c].x, ai[c]);
+                    ar[KA + c] = fma(wmh, (double)a2r[c].y, ar[KA + c]);
+                    ai[KA + c] = fma(wmh, (double)a2i[c].y, ai[KA + c]);
+                }
+            } else {
+                float a32r[KH], a32i[KH];
+#pragma unroll
+                for (int j = 0; j < KH; ++j) { a32r[j] = 0.0f; a32i[j] = 0.0f; }
+                inner_block<KH, TPL, PE_UNROLL, float, float2, float>(sr, si, a32r, a32i, sm, sm.B32, sm.tab_w32, 1.0f,
+                                                                     1.0f, fwd, Lin, c0, h, gmask);
+#pragma unroll
+                for (int j = 0; j < KH; ++j) {
+                    ar[j] = fma(wmh, (double)a32r[j], ar[j]);
+                    ai[j] = fma(wmh, (double)a32i[j], ai[j]);
+                }
+            }
         }
     }
     reduce_to_P<KH, TPL>(ar, ai, sm, c0);
@@ -722,7 +848,9 @@ template <int TPL, int KPM, bool MIXED>
 __device__ __forceinline__ void cofactor_step(Smem& sm, const double2* A, int64_t rs, int64_t cs, int K1, int K) {
     if (threadIdx.x < 32) plan_step(sm, K1, K, blockDim.x / TPL * sm.lane_mult, MIXED ? MIXED_LIN : LIN_MAX, MID_MAX);
     __syncthreads();
-    prepare_step(sm, A, rs, cs, MIXED);
+    // paired FP32 sweeps (mixed form, 1- and 2-thread lanes): columns per thread of the dispatched tier
+    const int kh = (MIXED && PE_PAIR32 && TPL <= 2) ? ((K + 3) / 4 * 4) / TPL : 0;
+    prepare_step(sm, A, rs, cs, MIXED, kh);
     __syncthreads();
     if constexpr (MIXED) dispatch_mixed<TPL, KPM>(sm, K);
     else dispatch_f64<TPL, KPM>(sm, K);

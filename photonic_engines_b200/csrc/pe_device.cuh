@@ -82,7 +82,8 @@ struct Smem {
     Plan plan;
     double2 P[MAXN];               // cofactors of the step (scaled)
     double2 B[MAXN][MAXN];         // B[kd][j] = A[drow_kd, col_j], padded columns zero
-    float2 B32[MAXN][MAXN];        // 2 * B in float32 (the mixed form's Gray update)
+    alignas(16) float2 B32[MAXN][MAXN];   // 2 * B in float32 (the mixed form's Gray update); paired
+                                   // sweeps read each row as float4 slots (see prepare_step)
     double tab_w[LIN_MAX];         // inner weight prod (-1)^v C(M, v) at inner index t
     float tab_w32[LIN_MAX];
     double tab_wm[MID_MAX];        // middle weight at middle index
