@@ -71,7 +71,7 @@ DEFAULT_BLOCK = 128          # the library's CTA size when the caller passes 0 (
 def default_tpl(n: int, precision: str) -> int:
     """Threads per Gray lane the library picks when the caller passes 0 (fock_api.cu default_tpl)."""
     kpm = next((k for k in (8, 16, 20, 24, 28, 32) if n <= k), 32)
-    if kpm <= 8 or (precision == "f64" and kpm <= 20):
+    if kpm <= 8 or (precision == "f64" and kpm == 20):
         return 1
     return 2 if kpm <= 24 else 4
 

@@ -63,12 +63,12 @@ void* find_cofactor_kernel(int mixed, int tpl, int kpm) {
     return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_cof[mixed][ti][ki];
 }
 
-// Threads per Gray lane when the caller passes 0: one-thread lanes (no exchange of partial products)
-// wherever their registers fit — up to 20 columns in FP64, whose variants run 128-thread CTAs with 255
-// registers — two-thread lanes up to 24 columns, four beyond.
+// Threads per Gray lane when the caller passes 0 (measured at m = 400, 2 000 streams): one-thread lanes
+// up to 8 columns, and for FP64 chains of 17-20 photons (no exchange of partial products; those variants
+// run 128-thread CTAs with 255 registers); two-thread lanes up to 24 columns, four beyond.
 static int default_tpl(int kpm, int precision) {
     if (kpm <= 8) return 1;
-    if (precision == PE_PRECISION_F64 && kpm <= 20) return 1;
+    if (precision == PE_PRECISION_F64 && kpm == 20) return 1;
     return kpm <= 24 ? 2 : 4;
 }
 
