@@ -28,6 +28,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_PHOT, M_MODES, SHOTS, USEED = 20, 400, 2000, 1002
+# DRAM bytes (read + write) of one chain launch on this workload, from one ncu capture of each form
+# (dram__bytes_read.sum + dram__bytes_write.sum, `--profile-launch f64|mixed`); the algorithmic bytes
+# (16 m k + 16 k^2 per sample and step, 2.78 GB per launch) are served from L2 and shared memory.
+DRAM_BYTES_PER_LAUNCH = {"f64": 1.038e6 + 0.067e6, "mixed": 1.908e6 + 0.177e6}
 METRIC = "samples/s n=20 m=400: mixed-precision vs FP64 on B200, marginal err<=1e-6"
 WORKLOAD = "fock n=20 photons (modes 0..19), m=400, 2000 shots/step, lossless, Haar U (seeded QR)"
 
@@ -252,12 +256,14 @@ def run_b200(args):
     if rank == 0:
         mx, f64 = res["mixed"], res["f64"]
 
-        def roof(r, peak, unit_bound):
+        def roof(r, peak, unit_bound, form):
             flops_launch = statistics.mean(w["flops"] for w in r["work"])
             dur = statistics.mean(r["kern_ms"]) * 1e-3
             achieved = flops_launch / dur / 1e12
             return {"bound": unit_bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": None,
+                    "frac": achieved / peak, "traffic": DRAM_BYTES_PER_LAUNCH[form],
+                    "traffic_unit": "bytes per launch (ncu dram read + write, one capture)",
+                    "algorithmic_bytes_per_launch": statistics.mean(w["bytes"] for w in r["work"]),
                     "peak_source": "measured live by pe_pipe_probe (FMA chains) on this GPU",
                     "flops_per_launch": flops_launch, "launch_ms": dur * 1e3}
 
@@ -271,9 +277,9 @@ def run_b200(args):
             "config": {"workload": WORKLOAD, "n": N_PHOT, "m": M_MODES, "shots_per_step": SHOTS,
                        "precision": "mixed", "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"replicas x{ws}"},
-            "roofline": roof(mx, peak32, "fp32"),
+            "roofline": roof(mx, peak32, "fp32", "mixed"),
             "fp64": {"value": v64, "ms_per_step": f64["elapsed"] / args.steps * 1e3,
-                     "roofline": roof(f64, peak64, "fp64"), "clocks": f64["clocks"]},
+                     "roofline": roof(f64, peak64, "fp64", "f64"), "clocks": f64["clocks"]},
             "mixed_over_fp64": value / v64,
             "max_marginal_rel_err": max_err, "picks_equal_fp64": picks_equal,
             "addends_per_sample": statistics.mean(w["addends"] for w in mx["work"]) / SHOTS,
