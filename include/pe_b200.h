@@ -147,6 +147,27 @@ int pe_fock_chain_adaptive(int precision, const double* d_acol, const int64_t* d
 size_t pe_adaptive_workspace_bytes(int64_t S, int nch);
 
 /*
+ * Emitter inputs (EmitterMPS with emitter dimension chi = 2, 1 or 2 labels per photon): one step of the
+ * generalised chain rule, the matrix-cofactor sum of photonic_engines/clifford/emitter_reference.py:280-305
+ * (matrix_cofactor_weights) as batched by emitter_sampler.py:150-175 (sample_torch) and by the reference's
+ * CUDA kernel emit_multi (cuda_emitter.py:511).  A lane is one stream and one pure term of its reduced
+ * state; lanes of a stream are contiguous (d_lstart / d_nlan per stream).
+ *   d_ut        [M][m] complex: d_ut[mode * m + rho] = U[rho, mode]
+ *   d_rows      [S][rows_stride] int64: the stream's k - 1 chosen output rows (chain order)
+ *   d_colmode   [S][k][L] int32: input mode of label l of the stream's j-th placed photon (slots sorted)
+ *   d_s0, d_f   [Tt][2] complex; d_mats [Tt][k][L][2][2] complex: the terms (s0_e, M~_e, f_e)
+ *   d_lane_term, d_lane_stream [nl] int64; d_lstart, d_nlan [S] int64
+ * Outputs: d_amp [nl][m] complex amplitudes, d_w [S][m] float64 weights (sum of |amp|^2 over the stream's
+ * lanes, in lane order).  k <= 24.  Workspace: pe_emitter_workspace_bytes() (status word).
+ */
+int pe_emitter_weights(const double* d_ut, int m, int M, const int64_t* d_rows, int rows_stride,
+                       const int32_t* d_colmode, int64_t S, int k, int L, int chi, const double* d_s0,
+                       const double* d_f, const double* d_mats, int64_t Tt, const int64_t* d_lane_term,
+                       const int64_t* d_lane_stream, const int64_t* d_lstart, const int64_t* d_nlan, int64_t nl,
+                       double* d_amp, double* d_w, void* d_workspace, size_t workspace_bytes, void* stream);
+size_t pe_emitter_workspace_bytes(void);
+
+/*
  * pe_fock_chain without a workspace argument: the same chains and outputs, for callers that cannot
  * allocate device memory when they sample (a host callback or other context where CUDA allocation is not
  * allowed, a serving process whose device memory all belongs to its own arena, a foreign-language

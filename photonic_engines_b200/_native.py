@@ -14,6 +14,10 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.environ.get("PE_LIB", os.path.join(_HERE, "libpe_b200.so"))
 
 PE_OK = 0
+PE_ERR_ARG = -1
+PE_ERR_SIZE = -2
+PE_ERR_CUDA = -3
+PE_ERR_DEVICE = -4
 PE_PRECISION_F64 = 0
 PE_PRECISION_MIXED = 1
 PE_MAX_PHOTONS = 32
@@ -62,6 +66,11 @@ def load() -> ctypes.CDLL:
                                          _i32, _i32, _vp]
     L.pe_adaptive_workspace_bytes.restype = ctypes.c_size_t
     L.pe_adaptive_workspace_bytes.argtypes = [_i64, _i32]
+    L.pe_emitter_weights.restype = _i32
+    L.pe_emitter_weights.argtypes = [_vp, _i32, _i32, _vp, _i32, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _vp, _i64, _vp,
+                                     _vp, _vp, _vp, _i64, _vp, _vp, _vp, ctypes.c_size_t, _vp]
+    L.pe_emitter_workspace_bytes.restype = ctypes.c_size_t
+    L.pe_emitter_workspace_bytes.argtypes = []
     L.pe_fock_chain_noalloc.restype = _i32
     L.pe_fock_chain_noalloc.argtypes = [_i32, _vp, _vp, _vp, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i32, _vp, _vp, _vp,
                                         _vp, _vp, _vp, _vp, _i32, _vp, _i32, _vp, _i32, _i32, _i32, _vp]
@@ -84,7 +93,8 @@ def load() -> ctypes.CDLL:
 # every symbol the C header declares (checked by the CPU test that loads the library)
 EXPORTED = ("pe_version", "pe_max_modes", "pe_chain_workspace_bytes", "pe_fock_chain", "pe_fock_chain_noalloc",
             "pe_fock_chain_split", "pe_chain_split_workspace_bytes", "pe_fock_chain_warp",
-            "pe_fock_chain_adaptive", "pe_adaptive_workspace_bytes",
+            "pe_fock_chain_adaptive", "pe_adaptive_workspace_bytes", "pe_emitter_weights",
+            "pe_emitter_workspace_bytes",
             "pe_cofactors_rows", "pe_partition_shots", "pe_scatter_occupations", "pe_pipe_probe", "pe_read_status",
             "pe_status_string")
 

@@ -69,7 +69,7 @@ def build(jobs: int | None = None, verbose: bool = False, ptxas_info: bool = Fal
                           f"-DPE_TPL={tpl}", f"-DPE_KPM={kpm}", *variant_flags(mx, tpl, kpm), "-c",
                           os.path.join(CSRC, "fock_inst.cu"), "-o", obj])
     extra = []
-    for name in ("fock_api", "fock_batch"):
+    for name in ("fock_api", "fock_batch", "emitter"):
         obj = os.path.join(OBJ, f"{name}.o")
         extra.append(obj)
         if _stale(obj, deps):

@@ -1,0 +1,230 @@
+"""Exact sampling of EmitterMPS inputs (one emitter of dimension chi = 2 emitting n photons) on B200.
+
+    emitter_sample(state, U, shots, generator)     the reference's `clifford.emitter_sample` (lossless)
+
+The generalised Clifford & Clifford chain rule (photonic_engines/clifford/emitter_reference.py,
+emitter_sampler.py): photon order sigma uniform; at step k the k placed photons T = sorted(sigma[:k]) have
+a reduced state that is a sum of R pure MPS terms (the gap channels between placed photons, each
+decomposed into orthogonal Kraus operators); output mode rho is drawn with weight
+w(rho) = sum_e |amp_e(rho)|^2, amp_e(rho) = sum_c sum_l U[rho, mode(c, l)] Tr(M~_{e,c,l} K_{e,c}), the
+matrix cofactors K_{e,c} being Glynn sums over delta with chi x chi matrix chains.
+
+Here the term decomposition (small SVDs, cached per (T, final spin)) runs on the host as in the
+reference; the per-step sum over every (stream, term) lane and every sign vector runs in one launch of
+`pe_emitter_weights` (csrc/emitter.cu), and the draw consumes the caller's generator exactly as the
+reference's torch sampler does (final spin, photon order, one multinomial per step), so a seeded CPU
+generator gives the reference's samples.
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+
+from .. import _native as N
+from ..states import EmitterMPS
+
+C128 = torch.complex128
+_TOL = 1e-12
+
+
+def final_spin_distribution(state: EmitterMPS) -> torch.Tensor:
+    """p(s_f) of a traced emitter: the diagonal of rho_n = E_n ... E_1(|s0><s0|), E_k(rho) = sum_l M_kl rho
+    M_kl^dag (emitter_reference.py:54-65)."""
+    ops = torch.as_tensor(state.ops, dtype=C128)
+    s0 = torch.as_tensor(state.s0, dtype=C128).reshape(-1)
+    rho = torch.outer(s0, s0.conj())
+    for k in range(state.n):
+        rho = torch.einsum("lts,su,lvu->tv", ops[k], rho, ops[k].conj())
+    return rho.diagonal().real.clamp_min(0)
+
+
+def _span_rows(V: torch.Tensor) -> torch.Tensor:
+    """Rows W with W^dag W = V^dag V and as few rows as the rank of V (SVD, relative cut 1e-12)."""
+    _, sv, vh = torch.linalg.svd(V, full_matrices=False)
+    keep = _TOL * max(1.0, float(sv[0])) < sv if sv.numel() else _TOL < sv
+    return sv[keep].unsqueeze(1) * vh[keep]
+
+
+def _kraus(A: torch.Tensor) -> torch.Tensor:
+    """Orthogonal Kraus operators [R, chi, chi] of the channel sum_x A_x . A_x^dag (A [N, chi, chi])."""
+    n_, chi, _ = A.shape
+    return _span_rows(A.reshape(n_, chi * chi)).reshape(-1, chi, chi)
+
+
+def gap_terms(state: EmitterMPS, T, final=None):
+    """Pure terms of the reduced state of the photons in slots T (emitter_reference.py:190-277):
+    (kept slots sorted(T), s0 [R, chi], mats [R, k, L, chi, chi], f [R, chi]) with
+    rho_T = sum_e |psi_e><psi_e|, psi_e(x) = <f_e| M~_{e,k-1,x} ... M~_{e,0,x} |s0_e>.  The photons before
+    the first placed one act on |s0> and those after the last on <final| (their images are reduced to an
+    orthogonal set after every slot); a run of unplaced photons between two placed ones is a channel whose
+    Kraus operators multiply the earlier placed photon's operators on the left.  Zero-norm terms dropped."""
+    n, chi = state.n, state.chi
+    ops = torch.as_tensor(state.ops, dtype=C128)
+    s0 = torch.as_tensor(state.s0, dtype=C128)
+    f = torch.as_tensor(state.final if final is None else final, dtype=C128)
+    kept = sorted(int(t) for t in T)
+    k = len(kept)
+    V = s0.unsqueeze(0)                                                   # images of |s0>
+    for j in range(kept[0]):
+        V = _span_rows(torch.einsum("lts,rs->rlt", ops[j], V).reshape(-1, chi))
+    W = f.conj().unsqueeze(0)                                             # images of <f|
+    for j in range(n - 1, kept[-1], -1):
+        W = _span_rows(torch.einsum("rs,lst->rlt", W, ops[j]).reshape(-1, chi))
+    f_terms = W.conj()
+    gaps = []
+    for a, b in zip(kept, kept[1:]):
+        if b == a + 1:
+            gaps.append(None)
+            continue
+        K = torch.eye(chi, dtype=C128).unsqueeze(0)
+        for j in range(a + 1, b):
+            K = _kraus(torch.einsum("lts,rsu->rltu", ops[j], K).reshape(-1, chi, chi))
+        gaps.append(K)
+    r0, rf = V.shape[0], f_terms.shape[0]
+    ranks = [1 if K is None else K.shape[0] for K in gaps]
+    R = r0 * rf * math.prod(ranks)
+    mats = ops[kept].unsqueeze(0).repeat(R, 1, 1, 1, 1)
+    rem = torch.arange(R)
+    choice = []
+    for rk in reversed(ranks):                                            # term index = (i0, if, g_1 .. g_{k-1})
+        choice.append(rem % rk)
+        rem = rem // rk
+    choice = choice[::-1]
+    i_f, i_0 = rem % rf, rem // rf
+    for gi, K in enumerate(gaps):
+        if K is not None:
+            mats[:, gi] = torch.einsum("rts,rlsu->rltu", K[choice[gi]], mats[:, gi])
+    s0_all, f_all = V[i_0], f_terms[i_f]
+    v = torch.einsum("rs,rt->rst", s0_all, s0_all.conj()).reshape(R, chi * chi)
+    for j in range(k):
+        E = torch.einsum("rlts,rluv->rtusv", mats[:, j], mats[:, j].conj()).reshape(R, chi * chi, chi * chi)
+        v = torch.einsum("rab,rb->ra", E, v)
+    fv = torch.einsum("rs,rt->rst", f_all, f_all.conj()).reshape(R, chi * chi)
+    norm2 = torch.einsum("ra,ra->r", fv.conj(), v).real
+    scale = (f_all.abs() ** 2).sum(1) * (s0_all.abs() ** 2).sum(1)
+    keep = norm2 > 1e-14 * scale.clamp_min(1.0)
+    return kept, s0_all[keep].contiguous(), mats[keep].contiguous(), f_all[keep].contiguous()
+
+
+class _Terms:
+    """gap_terms per (sorted T, final id), cached."""
+
+    def __init__(self, state: EmitterMPS):
+        self.state = state
+        self.finals = [None] if state.final is not None else list(torch.eye(state.chi, dtype=C128))
+        self.cache: dict = {}
+
+    def get(self, T: tuple, fid: int):
+        key = (T, fid)
+        if key not in self.cache:
+            self.cache[key] = gap_terms(self.state, T, self.finals[fid])[1:]
+        return self.cache[key]
+
+
+def step_weights(U_t: torch.Tensor, state: EmitterMPS, Tsorted: torch.Tensor, rows: torch.Tensor, fid: torch.Tensor,
+                 terms: _Terms, k: int) -> tuple[torch.Tensor, int]:
+    """(w [S, m] float64 on U's device, lanes) of step k for every stream: Tsorted [S, k] placed slots
+    (sorted), rows [S, >= k - 1] the chosen rows (device), fid [S] final-spin ids.  One launch of
+    pe_emitter_weights over all (stream, term) lanes."""
+    dev = U_t.device
+    m = U_t.shape[0]
+    S = Tsorted.shape[0]
+    keys = torch.cat([Tsorted, fid.unsqueeze(1)], dim=1)
+    uniq, inverse = torch.unique(keys, dim=0, return_inverse=True)
+    s0_l, f_l, mats_l, R_u = [], [], [], []
+    for key in uniq.tolist():
+        s0, mats, f = terms.get(tuple(key[:k]), key[k])
+        s0_l.append(s0)
+        mats_l.append(mats)
+        f_l.append(f)
+        R_u.append(s0.shape[0])
+    R_u = torch.tensor(R_u, dtype=torch.int64)
+    base_u = torch.cumsum(R_u, 0) - R_u
+    nlan = R_u[inverse]                                                    # lanes per stream
+    lstart = torch.cumsum(nlan, 0) - nlan
+    nl = int(nlan.sum())
+    lane_stream = torch.repeat_interleave(torch.arange(S), nlan)
+    lane_term = base_u[inverse][lane_stream] + (torch.arange(nl) - lstart[lane_stream])
+    modes = torch.tensor([list(mk) for mk in state.modes], dtype=torch.int32)          # [n, L]
+    colmode = modes[Tsorted].contiguous()                                             # [S, k, L]
+    s0 = torch.cat(s0_l).to(dev)
+    f = torch.cat(f_l).to(dev)
+    mats = torch.cat(mats_l).to(dev)
+    L = state.num_labels
+    ut = torch.view_as_real(U_t.transpose(0, 1).contiguous().to(C128)).contiguous()      # [M][m]
+    amp = torch.empty(max(nl, 1), m, dtype=C128, device=dev)
+    w = torch.empty(S, m, dtype=torch.float64, device=dev)
+    ws = torch.empty(int(N.load().pe_emitter_workspace_bytes()), dtype=torch.uint8, device=dev)
+    tensors = [t.to(dev).contiguous() for t in (colmode, lane_term, lane_stream, lstart, nlan)]
+    colmode_d, lane_term_d, lane_stream_d, lstart_d, nlan_d = tensors
+    rows_d = rows.to(dev, torch.int64).contiguous()
+    rc = N.load().pe_emitter_weights(N.ptr(ut), m, int(U_t.shape[1]), N.ptr(rows_d), int(rows_d.shape[1]),
+                                     N.ptr(colmode_d), S, k, L, state.chi, N.ptr(torch.view_as_real(s0)),
+                                     N.ptr(torch.view_as_real(f)), N.ptr(torch.view_as_real(mats)), int(s0.shape[0]),
+                                     N.ptr(lane_term_d), N.ptr(lane_stream_d), N.ptr(lstart_d), N.ptr(nlan_d), nl,
+                                     N.ptr(torch.view_as_real(amp)), N.ptr(w), N.ptr(ws), int(ws.numel()),
+                                     N.stream_handle(dev))
+    N.check(rc, "pe_emitter_weights")
+    st, det = N.read_status(ws)
+    if st != 0:
+        raise N.NativeError(f"pe_emitter_weights: device-side index error at {det}")
+    return w, nl
+
+
+def emitter_sample(state: EmitterMPS, U: torch.Tensor, shots: int, generator: torch.Generator | None = None,
+                   backend: str = "b200", return_stats: bool = False, loss=None, indist=None, **kw):
+    """Exact samples [shots, m] int64 (on U's device) of the EmitterMPS `state` through U (CUDA).
+
+    Keeps the reference's call (photonic_engines/clifford/__init__.py:36-60) and the random-number use of
+    its exact torch sampler (emitter_sampler.py:100-180): a final emitter spin per stream from p(s_f) when
+    the emitter is traced out (multinomial on `generator`), the photon order argsort(rand(shots, n)), then
+    one multinomial draw per step from the normalised weights — with a CPU generator seeded alike, the
+    same samples.  chi = 2 and 1 or 2 labels per photon (the reference GPU kernel's range); loss and
+    partial distinguishability are not part of this path."""
+    if backend not in ("b200", "triton", "torch", "cuda"):
+        raise ValueError(f"unknown backend {backend!r}")
+    if loss is not None and float(loss) < 1.0 or indist is not None:
+        raise NotImplementedError("emitter_sample: loss / partial distinguishability are not available on this path")
+    state.require_uniform_labels("emitter_sample")
+    if state.chi != 2 or state.num_labels > 2:
+        raise NotImplementedError("emitter_sample: emitter dimension 2 with 1 or 2 labels per photon only")
+    N.require_cuda(U, "U")
+    dev = U.device
+    U_t = torch.as_tensor(U).to(dev, C128)
+    m, n = U_t.shape[0], state.n
+    if m != state.m:
+        raise ValueError(f"U is {m} x {m}, the state has m = {state.m}")
+    if n > 24:
+        raise ValueError("emitter_sample: at most 24 photons")
+    S = int(shots)
+    if generator is None:
+        generator = torch.Generator().manual_seed(0)
+    gdev = generator.device
+    if state.final is None:
+        pf = final_spin_distribution(state)
+        fid = torch.multinomial(pf / pf.sum(), S, replacement=True, generator=generator).cpu()
+    else:
+        fid = torch.zeros(S, dtype=torch.long)
+    sigma = torch.argsort(torch.rand((S, n), generator=generator, device=gdev), dim=1).cpu()
+    rows = torch.zeros((S, n), dtype=torch.long)
+    rows_d = torch.zeros((S, max(n, 1)), dtype=torch.int64, device=dev)
+    terms = _Terms(state)
+    stats = {"R": []}                                                    # mean lanes (pure terms) per stream
+    for k in range(1, n + 1):
+        Tsorted = torch.sort(sigma[:, :k], dim=1).values
+        w, nl = step_weights(U_t, state, Tsorted, rows_d, fid, terms, k)
+        w = w.cpu()
+        w = w.clamp_min(0)
+        w = w / w.sum(dim=1, keepdim=True)
+        rho = torch.multinomial(w, 1, generator=generator).squeeze(1)
+        rows[:, k - 1] = rho
+        rows_d[:, k - 1] = rho.to(dev)
+        stats["R"].append(nl / max(S, 1))
+    occ = torch.zeros((S, m), dtype=torch.long)
+    occ.scatter_add_(1, rows, torch.ones_like(rows))
+    occ = occ.to(dev)
+    return (occ, stats) if return_stats else occ
+
+
+__all__ = ["emitter_sample", "final_spin_distribution", "gap_terms", "step_weights"]

@@ -1,0 +1,300 @@
+// Emitter inputs (EmitterMPS, chi = 2): the matrix-cofactor step of the generalised Clifford chain rule
+// on B200.  Per lane (a stream and one pure term of its reduced state) and per Glynn sign vector delta in
+// {+1} x {-1, +1}^(k-2) of the k-1 chosen rows:
+//   colsum_{j,l} = sum_i delta_i U[row_i, mode(j, l)]                   (column sums, Gray-updated)
+//   G_j = sum_l colsum_{j,l} M_{j,l}                                     (2 x 2)
+//   q_c = f^dag G_{k-1} ... G_{c+1}     (backward, row vectors)   p_c = G_{c-1} ... G_0 s0  (forward)
+//   t_{c,l} += sign(delta) q_c M_{c,l} p_c                               (= Tr(M_{c,l} K_c))
+// then amp(rho) = 2^-(k-2) sum_c sum_l U[rho, mode(c, l)] t_{c,l} for every output mode rho, and the
+// stream's weight w(rho) = sum over its lanes of |amp(rho)|^2.  This is the reference's
+// matrix_cofactor_weights (photonic_engines/clifford/emitter_reference.py:280-305) and the step of
+// emitter_sampler.sample_torch (emitter_sampler.py:150-175), restated for one CTA per lane.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pe_b200.h"
+
+namespace pe_em {
+
+constexpr int CHI = 2;
+constexpr int THREADS = 128;
+constexpr int NWARP = THREADS / 32;
+constexpr int MAXK = 24;
+
+struct Params {
+    const double2* UT;          // [M][m]: UT[mode * m + rho] = U[rho, mode]
+    int m, M;
+    const int64_t* rows;        // [S][rows_stride]: the chosen rows, first k - 1 valid
+    int rows_stride;
+    const int32_t* colmode;     // [S][k][L]: input mode of label l of the stream's j-th slot (slots sorted)
+    int64_t S;
+    int k, L;
+    const double2* s0;          // [Tt][2]
+    const double2* f;           // [Tt][2]
+    const double2* mats;        // [Tt][k][L][2][2]
+    int64_t Tt;
+    const int64_t* lane_term;   // [nl]
+    const int64_t* lane_stream; // [nl]
+    int64_t nl;
+    double2* amp;               // [nl][m]
+    int* status;
+    long long* detail;
+};
+
+static __device__ __forceinline__ void record(int* status, long long* detail, int64_t x) {
+    if (atomicCAS(status, 0, PE_ERR_DEVICE) == 0) *detail = (long long)x;
+}
+static __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(fma(a.x, b.x, -(a.y * b.y)), fma(a.x, b.y, a.y * b.x));
+}
+static __device__ __forceinline__ double2 cmac(double2 acc, double2 a, double2 b) {   // acc + a b
+    return make_double2(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));
+}
+
+template <int KE, int NL>
+__global__ void __launch_bounds__(THREADS) emitter_amp_kernel(Params p) {
+    __shared__ double2 sM[KE][NL][CHI][CHI];
+    __shared__ double2 sU[KE][KE][NL];          // sU[i][j][l] = U[row_i, mode(j, l)], i < k - 1
+    __shared__ double2 red[NWARP][KE][NL];
+    __shared__ double2 sT[KE][NL];
+    __shared__ int sMode[KE][NL];
+    __shared__ int sRow[KE];
+    __shared__ int bad;
+    const int tid = threadIdx.x, lid = tid & 31, wid = tid >> 5;
+    const int k = p.k, kk = k - 1;
+    for (int64_t lane = blockIdx.x; lane < p.nl; lane += gridDim.x) {
+        if (tid == 0) bad = 0;
+        __syncthreads();
+        const int64_t s = p.lane_stream[lane], e = p.lane_term[lane];
+        if (s < 0 || s >= p.S || e < 0 || e >= p.Tt) {
+            if (tid == 0) record(p.status, p.detail, lane);
+            __syncthreads();
+            continue;
+        }
+        if (tid < k * NL) {
+            const int j = tid / NL, l = tid % NL;
+            const int md = p.colmode[(s * k + j) * p.L + l];
+            if (md < 0 || md >= p.M) atomicOr(&bad, 1);
+            else sMode[j][l] = md;
+        }
+        if (tid < kk) {
+            const int64_t r = p.rows[s * p.rows_stride + tid];
+            if (r < 0 || r >= p.m) atomicOr(&bad, 1);
+            else sRow[tid] = (int)r;
+        }
+        for (int idx = tid; idx < k * NL * CHI * CHI; idx += THREADS) {
+            const int j = idx / (NL * CHI * CHI), rem = idx % (NL * CHI * CHI);
+            const int l = rem / (CHI * CHI), ab = rem % (CHI * CHI);
+            sM[j][l][ab / CHI][ab % CHI] = p.mats[(e * k + j) * (int64_t)p.L * CHI * CHI + l * CHI * CHI + ab];
+        }
+        __syncthreads();
+        if (bad) {
+            if (tid == 0) record(p.status, p.detail, lane);
+            __syncthreads();
+            continue;
+        }
+        for (int idx = tid; idx < kk * k * NL; idx += THREADS) {
+            const int i = idx / (k * NL), rem = idx % (k * NL);
+            const int j = rem / NL, l = rem % NL;
+            sU[i][j][l] = p.UT[(int64_t)sMode[j][l] * p.m + sRow[i]];
+        }
+        __syncthreads();
+        const double2 s00 = p.s0[e * CHI], s01 = p.s0[e * CHI + 1];
+        const double2 f0 = p.f[e * CHI], f1 = p.f[e * CHI + 1];
+        const double2 fc0 = make_double2(f0.x, -f0.y), fc1 = make_double2(f1.x, -f1.y);
+
+        // this thread's contiguous block [t0, t1) of Gray indices over the k - 2 free signs
+        const int64_t D = kk >= 1 ? ((int64_t)1 << (kk - 1)) : 1;
+        int64_t t0, t1;
+        if (D >= THREADS) { const int64_t per = D / THREADS; t0 = tid * per; t1 = t0 + per; }
+        else { t0 = tid; t1 = tid < D ? tid + 1 : tid; }
+        double2 acc[KE][NL];
+#pragma unroll
+        for (int j = 0; j < KE; ++j)
+#pragma unroll
+            for (int l = 0; l < NL; ++l) acc[j][l] = make_double2(0.0, 0.0);
+        if (t0 < t1) {
+            double2 cs[KE][NL];
+            uint64_t g = (uint64_t)(t0 ^ (t0 >> 1));
+#pragma unroll
+            for (int j = 0; j < KE; ++j)
+#pragma unroll
+                for (int l = 0; l < NL; ++l) {
+                    double2 x = make_double2(kk == 0 ? 1.0 : 0.0, 0.0);
+                    if (j < k) {
+                        for (int i = 0; i < kk; ++i) {
+                            const double d = (i == 0 || !((g >> (i - 1)) & 1)) ? 1.0 : -1.0;
+                            x.x = fma(d, sU[i][j][l].x, x.x);
+                            x.y = fma(d, sU[i][j][l].y, x.y);
+                        }
+                    }
+                    cs[j][l] = x;
+                }
+            double sign = (__popcll(g) & 1) ? -1.0 : 1.0;
+            for (int64_t t = t0; t < t1; ++t) {
+                if (t > t0) {                                   // Gray step into t: free bit b flips
+                    const int b = __ffsll((long long)t) - 1;
+                    g ^= (uint64_t)1 << b;
+                    const double d2 = ((g >> b) & 1) ? -2.0 : 2.0;   // 2 * new delta of row b + 1
+                    const int i = b + 1;
+#pragma unroll
+                    for (int j = 0; j < KE; ++j)
+#pragma unroll
+                        for (int l = 0; l < NL; ++l)
+                            if (j < k) {
+                                cs[j][l].x = fma(d2, sU[i][j][l].x, cs[j][l].x);
+                                cs[j][l].y = fma(d2, sU[i][j][l].y, cs[j][l].y);
+                            }
+                    sign = -sign;
+                }
+                // backward: q_c (stored), u <- u G_c
+                double2 q0[KE], q1[KE];
+                double2 u0 = fc0, u1 = fc1;
+#pragma unroll
+                for (int c = KE - 1; c >= 0; --c) {
+                    if (c < k) {
+                        q0[c] = u0; q1[c] = u1;
+                        double2 n0 = make_double2(0.0, 0.0), n1 = make_double2(0.0, 0.0);
+#pragma unroll
+                        for (int l = 0; l < NL; ++l) {
+                            // z = u M_{c,l} (row vector), then u' += colsum z
+                            const double2 z0 = cmac(cmul(u0, sM[c][l][0][0]), u1, sM[c][l][1][0]);
+                            const double2 z1 = cmac(cmul(u0, sM[c][l][0][1]), u1, sM[c][l][1][1]);
+                            n0 = cmac(n0, cs[c][l], z0);
+                            n1 = cmac(n1, cs[c][l], z1);
+                        }
+                        u0 = n0; u1 = n1;
+                    }
+                }
+                // forward: y = M_{c,l} v, t_{c,l} += sign q_c . y, v <- sum_l colsum y
+                double2 v0 = s00, v1 = s01;
+#pragma unroll
+                for (int c = 0; c < KE; ++c) {
+                    if (c < k) {
+                        double2 n0 = make_double2(0.0, 0.0), n1 = make_double2(0.0, 0.0);
+#pragma unroll
+                        for (int l = 0; l < NL; ++l) {
+                            const double2 y0 = cmac(cmul(sM[c][l][0][0], v0), sM[c][l][0][1], v1);
+                            const double2 y1 = cmac(cmul(sM[c][l][1][0], v0), sM[c][l][1][1], v1);
+                            const double2 dt = cmac(cmul(q0[c], y0), q1[c], y1);
+                            acc[c][l].x = fma(sign, dt.x, acc[c][l].x);
+                            acc[c][l].y = fma(sign, dt.y, acc[c][l].y);
+                            n0 = cmac(n0, cs[c][l], y0);
+                            n1 = cmac(n1, cs[c][l], y1);
+                        }
+                        v0 = n0; v1 = n1;
+                    }
+                }
+            }
+        }
+        // deterministic reduction: warp butterflies, then the warps in order
+#pragma unroll
+        for (int j = 0; j < KE; ++j)
+#pragma unroll
+            for (int l = 0; l < NL; ++l) {
+                double2 x = acc[j][l];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    x.x += __shfl_xor_sync(0xffffffffu, x.x, o);
+                    x.y += __shfl_xor_sync(0xffffffffu, x.y, o);
+                }
+                if (lid == 0 && j < k) red[wid][j][l] = x;
+            }
+        __syncthreads();
+        const double norm = kk >= 1 ? ldexp(1.0, -(kk - 1)) : 1.0;
+        if (tid < k * NL) {
+            const int j = tid / NL, l = tid % NL;
+            double2 x = make_double2(0.0, 0.0);
+            for (int w = 0; w < NWARP; ++w) { x.x += red[w][j][l].x; x.y += red[w][j][l].y; }
+            sT[j][l] = make_double2(x.x * norm, x.y * norm);
+        }
+        __syncthreads();
+        for (int rho = tid; rho < p.m; rho += THREADS) {
+            double2 a = make_double2(0.0, 0.0);
+            for (int c = 0; c < k; ++c)
+#pragma unroll
+                for (int l = 0; l < NL; ++l) a = cmac(a, p.UT[(int64_t)sMode[c][l] * p.m + rho], sT[c][l]);
+            p.amp[lane * p.m + rho] = a;
+        }
+        __syncthreads();
+    }
+}
+
+// w[s][rho] = sum over the stream's lanes lstart[s] .. lstart[s] + nlan[s] - 1, in order, of |amp|^2.
+__global__ void emitter_weights_kernel(const double2* __restrict__ amp, const int64_t* __restrict__ lstart,
+                                       const int64_t* __restrict__ nlan, int64_t S, int m, int64_t nl, double* w,
+                                       int* status, long long* detail) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= S * m) return;
+    const int64_t s = idx / m;
+    const int rho = (int)(idx % m);
+    const int64_t a = lstart[s], b = a + nlan[s];
+    if (a < 0 || nlan[s] < 0 || b > nl) {
+        if (rho == 0) record(status, detail, s);
+        w[idx] = 0.0;
+        return;
+    }
+    double x = 0.0;
+    for (int64_t lane = a; lane < b; ++lane) {
+        const double2 v = amp[lane * m + rho];
+        x = fma(v.x, v.x, fma(v.y, v.y, x));
+    }
+    w[idx] = x;
+}
+
+template <int KE, int NL>
+static int launch_amp(const Params& p, cudaStream_t st) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emitter_amp_kernel<KE, NL>, THREADS, 0) != cudaSuccess)
+        return PE_ERR_CUDA;
+    if (per < 1) return PE_ERR_SIZE;
+    int64_t grid = (int64_t)sms * per;
+    if (grid > p.nl) grid = p.nl;
+    emitter_amp_kernel<KE, NL><<<(unsigned)grid, THREADS, 0, st>>>(p);
+    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+}
+
+}  // namespace pe_em
+
+using namespace pe_em;
+
+extern "C" size_t pe_emitter_workspace_bytes(void) { return 256; }
+
+extern "C" int pe_emitter_weights(const double* d_ut, int m, int M, const int64_t* d_rows, int rows_stride,
+                                  const int32_t* d_colmode, int64_t S, int k, int L, int chi, const double* d_s0,
+                                  const double* d_f, const double* d_mats, int64_t Tt, const int64_t* d_lane_term,
+                                  const int64_t* d_lane_stream, const int64_t* d_lstart, const int64_t* d_nlan,
+                                  int64_t nl, double* d_amp, double* d_w, void* d_workspace, size_t workspace_bytes,
+                                  void* stream) {
+    if (chi != CHI) return PE_ERR_SIZE;
+    if (L < 1 || L > 2 || k < 1 || k > MAXK) return PE_ERR_SIZE;
+    if (m < 1 || M < 1 || S < 0 || Tt < 0 || nl < 0 || rows_stride < (k > 1 ? k - 1 : 0)) return PE_ERR_ARG;
+    if (!d_ut || !d_colmode || !d_s0 || !d_f || !d_mats || !d_lane_term || !d_lane_stream || !d_lstart || !d_nlan ||
+        !d_amp || !d_w || !d_workspace || (k > 1 && !d_rows))
+        return PE_ERR_ARG;
+    if (workspace_bytes < 256) return PE_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(d_workspace, 0, 256, st) != cudaSuccess) return PE_ERR_CUDA;
+    if (S == 0) return PE_OK;
+    Params p;
+    p.UT = (const double2*)d_ut; p.m = m; p.M = M; p.rows = d_rows; p.rows_stride = rows_stride;
+    p.colmode = d_colmode; p.S = S; p.k = k; p.L = L;
+    p.s0 = (const double2*)d_s0; p.f = (const double2*)d_f; p.mats = (const double2*)d_mats; p.Tt = Tt;
+    p.lane_term = d_lane_term; p.lane_stream = d_lane_stream; p.nl = nl; p.amp = (double2*)d_amp;
+    p.status = (int*)((char*)d_workspace + 8);
+    p.detail = (long long*)((char*)d_workspace + 16);
+    int rc = PE_OK;
+    if (nl > 0) {
+        if (k <= 8) rc = L == 1 ? launch_amp<8, 1>(p, st) : launch_amp<8, 2>(p, st);
+        else if (k <= 16) rc = L == 1 ? launch_amp<16, 1>(p, st) : launch_amp<16, 2>(p, st);
+        else rc = L == 1 ? launch_amp<24, 1>(p, st) : launch_amp<24, 2>(p, st);
+        if (rc != PE_OK) return rc;
+    }
+    const int64_t total = S * (int64_t)m;
+    const int T = 256;
+    emitter_weights_kernel<<<(unsigned)((total + T - 1) / T), T, 0, st>>>((const double2*)d_amp, d_lstart, d_nlan, S, m,
+                                                                          nl, d_w, p.status, p.detail);
+    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+}

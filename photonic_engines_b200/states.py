@@ -38,3 +38,71 @@ class FockState:
 
     def norm_factor(self) -> float:
         return math.prod(math.factorial(x) for x in self.occupation)
+
+
+@dataclass(frozen=True)
+class EmitterMPS:
+    """Photons emitted one by one by a single emitter of dimension chi (the reference's `EmitterMPS`,
+    photonic_engines/states.py:306-420): at event k the emitter emits label l into input mode modes[k][l]
+    and is acted on by ops[k, l]; the photonic amplitude of labels x is <final| ops[n-1, x_{n-1}] ...
+    ops[0, x_0] |s0>, or the emitter is traced out when `final` is None.
+
+    ops [n, L, chi, chi] complex; modes: n tuples of L_k <= L distinct input modes (all distinct across
+    events); s0 [chi]; m >= 1 + max mode; final [chi] or None.  Padded labels (l >= L_k) must have zero
+    operators."""
+
+    ops: object
+    modes: tuple
+    s0: object
+    m: int
+    final: object = None
+
+    def __post_init__(self):
+        import numpy as np
+        ops = np.asarray(self.ops, dtype=np.complex128)
+        if ops.ndim != 4 or ops.shape[2] != ops.shape[3]:
+            raise ValueError("ops must have shape [n, L, chi, chi]")
+        n, L, chi, _ = ops.shape
+        modes = tuple(tuple(int(x) for x in mk) for mk in self.modes)
+        if len(modes) != n or any(not 1 <= len(mk) <= L for mk in modes):
+            raise ValueError("modes must have shape [n][L_k] with 1 <= L_k <= L")
+        for k, mk in enumerate(modes):
+            if np.any(ops[k, len(mk):]):
+                raise ValueError(f"ops[{k}, {len(mk)}:] must be zero: event {k} has {len(mk)} labels")
+        flat = [x for mk in modes for x in mk]
+        if len(set(flat)) != len(flat):
+            raise ValueError("every (event, label) must use a distinct input mode")
+        if min(flat) < 0 or max(flat) >= int(self.m):
+            raise ValueError("mode index out of range")
+        s0 = np.asarray(self.s0, dtype=np.complex128).reshape(-1)
+        if s0.shape != (chi,):
+            raise ValueError("s0 must have length chi")
+        final = None if self.final is None else np.asarray(self.final, dtype=np.complex128).reshape(-1)
+        if final is not None and final.shape != (chi,):
+            raise ValueError("final must have length chi")
+        object.__setattr__(self, "ops", ops)
+        object.__setattr__(self, "modes", modes)
+        object.__setattr__(self, "s0", s0)
+        object.__setattr__(self, "final", final)
+        object.__setattr__(self, "m", int(self.m))
+
+    @property
+    def n(self) -> int:
+        return self.ops.shape[0]
+
+    @property
+    def num_labels(self) -> int:
+        return self.ops.shape[1]
+
+    @property
+    def chi(self) -> int:
+        return self.ops.shape[2]
+
+    @property
+    def is_ragged(self) -> bool:
+        return any(len(mk) < self.num_labels for mk in self.modes)
+
+    def require_uniform_labels(self, where: str):
+        """NotImplementedError for a chain whose events have different label counts."""
+        if self.is_ragged:
+            raise NotImplementedError(f"ragged label counts ({tuple(len(mk) for mk in self.modes)}): not in {where}")

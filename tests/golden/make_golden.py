@@ -2,7 +2,7 @@
 
 Run in a container where the reference project is importable (it is NOT needed at test time):
 
-    python tests/golden/make_golden.py /path/to/photonic-engines [philox steps chains adaptive]
+    python tests/golden/make_golden.py /path/to/photonic-engines [philox steps chains adaptive emitter]
 
 It imports the reference read-only and records, with CPU tensors and the Triton CPU interpreter:
 
@@ -18,6 +18,9 @@ It imports the reference read-only and records, with CPU tensors and the Triton 
                rows and surviving stream ids with the sigma / seeds the generator produced, and
                `fock_sample(..., prefix=, avoid=, keep_ids=True)` occupations and ids (sampler.py:57-182,
                367-460).
+  emitter.npz  EmitterMPS inputs (chi = 2): step weights of `emitter_reference.matrix_cofactor_weights`
+               (emitter_reference.py:280-305) and occupations drawn by the exact torch sampler
+               `emitter_sampler.sample_torch` (emitter_sampler.py:82-180) for seeded CPU generators.
   chains.npz   whole chains drawn by the reference's sampler: `_sample_streams`
                (sampler.py:391-460) rows [S, n] in chain order, plus the sigma and per-step seeds
                the generator produced, and `fock_sample` occupations with loss / partial
@@ -251,6 +254,60 @@ def make_adaptive():
     np.savez_compressed(os.path.join(HERE, "adaptive.npz"), **out)
 
 
+def _emitters():
+    """(name, state) pairs: random emitters (chi = 2, 1 or 2 labels, projected or traced) and caterpillar
+    states built by the reference's EmitterMPS.caterpillar (their arrays are what is stored)."""
+    import math
+    from photonic_engines import EmitterMPS, spin_gate
+    out = []
+    for name, n, L, seed, final in [("rand_n3_L2_f", 3, 2, 4, True), ("rand_n4_L2_t", 4, 2, 6, False),
+                                    ("rand_n4_L1_f", 4, 1, 8, True), ("rand_n5_L2_f", 5, 2, 10, True),
+                                    ("rand_n5_L1_t", 5, 1, 12, False)]:
+        rng = np.random.default_rng(seed)
+        ops = rng.normal(size=(n, L, 2, 2)) + 1j * rng.normal(size=(n, L, 2, 2))
+        modes = tuple(tuple(range(k * L, (k + 1) * L)) for k in range(n))
+        s0 = rng.normal(size=2) + 1j * rng.normal(size=2)
+        f = (rng.normal(size=2) + 1j * rng.normal(size=2)) if final else None
+        out.append((name, EmitterMPS(ops=ops, modes=modes, s0=s0, m=n * L + 1, final=f)))
+    gates = [spin_gate(math.pi / 2, 0)] + [spin_gate(math.pi / 2, p) for p in (math.pi, 0, 0.9, 0.3)]
+    out.append(("caterpillar_n5", EmitterMPS.caterpillar(5, gates)))
+    out.append(("caterpillar_n4_f", EmitterMPS.caterpillar(4, gates[:4], final=(0.6, 0.8j))))
+    return out
+
+
+def make_emitter():
+    from photonic_engines.clifford.emitter_reference import matrix_cofactor_weights
+    from photonic_engines.clifford.emitter_sampler import sample_torch
+    out = {}
+    for si, (name, st) in enumerate(_emitters()):
+        U = haar(st.m, 300 + si)
+        out[f"{name}__ops"] = np.asarray(st.ops)
+        out[f"{name}__modes"] = np.array([list(mk) for mk in st.modes])
+        out[f"{name}__s0"] = np.asarray(st.s0)
+        out[f"{name}__final"] = np.asarray(st.final) if st.final is not None else np.zeros(0, dtype=np.complex128)
+        out[f"{name}__m"] = np.array([st.m])
+        out[f"{name}__U"] = U.numpy()
+        rng = np.random.default_rng(50 + si)
+        Ts, rows_l, fins, ws = [], [], [], []
+        for _ in range(4):                                   # steps with k = 1 .. n placed photons
+            k = int(rng.integers(1, st.n + 1))
+            T = sorted(rng.choice(st.n, size=k, replace=False).tolist())
+            rows = rng.integers(0, st.m, size=k - 1).tolist()
+            fin = None if st.final is not None else torch.eye(2, dtype=torch.complex128)[int(rng.integers(0, 2))]
+            w, _ = matrix_cofactor_weights(U, st, T, rows, final=fin)
+            Ts.append(T + [-1] * (st.n - k)); rows_l.append(rows + [-1] * (st.n - k))
+            fins.append(-1 if fin is None else int(torch.argmax(fin.abs())))
+            ws.append(w.numpy())
+        out[f"{name}__step_T"] = np.array(Ts); out[f"{name}__step_rows"] = np.array(rows_l)
+        out[f"{name}__step_final"] = np.array(fins); out[f"{name}__step_w"] = np.array(ws)
+        shots, seed = 300, 7 + si
+        occ = sample_torch(st, U, shots, generator=torch.Generator().manual_seed(seed))
+        out[f"{name}__shots_seed"] = np.array([shots, seed])
+        out[f"{name}__occ"] = occ.numpy()
+        print(name, "emitter", tuple(occ.shape), flush=True)
+    np.savez_compressed(os.path.join(HERE, "emitter.npz"), **out)
+
+
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PE_REFERENCE", "")
     if not ref or not os.path.isdir(ref):
@@ -258,5 +315,6 @@ if __name__ == "__main__":
     sys.path.insert(0, ref)
     parts = sys.argv[2:] or ["philox", "steps", "chains", "adaptive"]
     for part in parts:
-        {"philox": make_philox, "steps": make_steps, "chains": make_chains, "adaptive": make_adaptive}[part]()
+        {"philox": make_philox, "steps": make_steps, "chains": make_chains, "adaptive": make_adaptive,
+         "emitter": make_emitter}[part]()
         print(part, "done", flush=True)

@@ -1,0 +1,115 @@
+"""EmitterMPS inputs on the host: the oracle pinned on the reference's own outputs (tests/golden/emitter.npz:
+step weights of emitter_reference.matrix_cofactor_weights and occupations drawn by emitter_sampler.
+sample_torch), the pure-term decomposition of the reduced state, and argument checks.  The reference's
+tests this follows: tests/clifford/test_emitter_reference.py:88-126, test_emitter_sampler.py:58-72."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN
+from oracle import emitter_oracle as EO
+from photonic_engines_b200.clifford import emitter_sample
+from photonic_engines_b200.clifford.emitter import final_spin_distribution, gap_terms
+from photonic_engines_b200.states import EmitterMPS
+
+EMIT = np.load(os.path.join(GOLDEN, "emitter.npz"))
+CASES = sorted({k.split("__")[0] for k in EMIT.files})
+FAST = [c for c in CASES if c not in ("caterpillar_n5", "rand_n5_L2_f")]      # oracle sampler under ~2 s
+
+
+def case(name):
+    z = {k.split("__")[1]: EMIT[k] for k in EMIT.files if k.startswith(name + "__")}
+    fin = z["final"]
+    st = EmitterMPS(ops=z["ops"], modes=tuple(tuple(int(x) for x in r) for r in z["modes"]), s0=z["s0"],
+                    m=int(z["m"][0]), final=fin if fin.size else None)
+    steps = []
+    for i in range(z["step_T"].shape[0]):
+        T = [int(t) for t in z["step_T"][i] if t >= 0]
+        rows = [int(r) for r in z["step_rows"][i] if r >= 0]
+        fv = None if st.final is not None else np.eye(2)[int(z["step_final"][i])]
+        steps.append((T, rows, fv, z["step_w"][i]))
+    return st, z["U"], steps, int(z["shots_seed"][0]), int(z["shots_seed"][1]), z["occ"]
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_density_oracle_reproduces_the_reference_step_weights(name):
+    st, U, steps, *_ = case(name)
+    for T, rows, fv, w in steps:
+        f = st.final if fv is None else fv
+        assert _rel(EO.candidate_weights(U, st.ops, st.modes, st.s0, f, T, rows), w) < 1e-12
+
+
+@pytest.mark.parametrize("name", FAST)
+def test_oracle_sampler_reproduces_the_reference_draws(name):
+    st, U, _, shots, seed, occ = case(name)
+    got = EO.sample(U, st.ops, st.modes, st.s0, st.final, shots, torch.Generator().manual_seed(seed))
+    assert (got == occ).all()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_pure_terms_give_the_reference_weights(name):
+    """The host decomposition into pure terms, summed by the oracle's matrix-cofactor restatement."""
+    st, U, steps, *_ = case(name)
+    for T, rows, fv, w in steps:
+        kept, s0, mats, f = gap_terms(st, T, None if fv is None else torch.as_tensor(fv, dtype=torch.complex128))
+        colmode = np.array([list(st.modes[j]) for j in kept])
+        assert _rel(EO.matrix_weights(U, colmode, rows, s0.numpy(), mats.numpy(), f.numpy()), w) < 1e-12
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_pure_terms_reconstruct_the_reduced_density(seed):
+    """sum_e |psi_e><psi_e| = rho_T of the placed photons (emitter_reference.gap_kraus_terms' contract)."""
+    rng = np.random.default_rng(seed)
+    n, L = 6, 2
+    ops = rng.normal(size=(n, L, 2, 2)) + 1j * rng.normal(size=(n, L, 2, 2))
+    st = EmitterMPS(ops=ops, modes=tuple(tuple(range(2 * k, 2 * k + 2)) for k in range(n)),
+                    s0=rng.normal(size=2) + 1j * rng.normal(size=2), m=2 * n,
+                    final=rng.normal(size=2) + 1j * rng.normal(size=2))
+    c = np.einsum("...s,s->...", EO.coefficient_tensor(st.ops, st.s0), np.conj(st.final))
+    for T in ([0, 3], [1, 2, 5], [4], [0, 2, 4, 5], list(range(6))):
+        kept, s0, mats, f = gap_terms(st, T)
+        rho = np.zeros((L ** len(T), L ** len(T)), dtype=np.complex128)
+        for e in range(s0.shape[0]):
+            psi = np.zeros([L] * len(T), dtype=np.complex128)
+            for x in np.ndindex(*psi.shape):
+                v = s0[e].numpy()
+                for j, xj in enumerate(x):
+                    v = mats[e, j, xj].numpy() @ v
+                psi[x] = np.conj(f[e].numpy()) @ v
+            psi = psi.reshape(-1)
+            rho += np.outer(psi, psi.conj())
+        want = EO.reduced_density(c, kept)
+        assert np.abs(rho - want).max() < 1e-10 * np.abs(want).max(), T
+
+
+def test_final_spin_distribution_matches_the_coefficient_tensor():
+    st, *_ = case("rand_n4_L2_t")
+    p = final_spin_distribution(st).numpy()
+    assert np.allclose(p, EO.final_distribution(st.ops, st.s0), rtol=1e-12)
+
+
+def test_emitter_state_checks():
+    ops = np.zeros((2, 2, 2, 2), dtype=np.complex128)
+    with pytest.raises(ValueError):
+        EmitterMPS(ops=ops, modes=((0, 1), (1, 2)), s0=[1, 0], m=4)             # a mode used twice
+    with pytest.raises(ValueError):
+        EmitterMPS(ops=ops, modes=((0, 1), (2, 3)), s0=[1, 0, 0], m=4)          # s0 of the wrong size
+    with pytest.raises(ValueError):
+        EmitterMPS(ops=ops, modes=((0, 1), (2, 5)), s0=[1, 0], m=4)             # mode out of range
+
+
+def test_emitter_sample_argument_checks():
+    st, U, *_ = case("rand_n3_L2_f")
+    U = torch.as_tensor(U)
+    with pytest.raises(NotImplementedError):
+        emitter_sample(st, U, 4, loss=0.5)
+    with pytest.raises(NotImplementedError):
+        emitter_sample(EmitterMPS(ops=np.zeros((2, 1, 3, 3)), modes=((0,), (1,)), s0=[1, 0, 0], m=3), U[:3, :3], 2)
+    with pytest.raises(ValueError):
+        emitter_sample(st, U, 4, backend="nope")
