@@ -450,6 +450,83 @@ def profile_launch(precision: str):
     torch.cuda.synchronize()
 
 
+def run_emitter(args):
+    """One JSON line for EmitterMPS inputs: the linear cluster state (caterpillar, spin_gate(pi/2, 0) at every
+    emission, emitter traced out) of n = 12 photons in m = 24 modes through a seeded Haar U, 512 shots per step
+    — the workload of the reference's bench/bench_emitter_sampler.py.  A step is one emitter_sample call
+    (host term decomposition, one pe_emitter_weights launch per photon, host draws); the kernel roofline is
+    against the live FP64 pipe peak; the CPU baseline runs the same matrix-cofactor sums in numpy
+    (oracle/emitter_oracle.py) on a bounded sample of streams."""
+    import math
+
+    import numpy as np
+    import torch
+
+    from oracle import emitter_oracle as EO
+    from photonic_engines_b200 import _native as NAT
+    from photonic_engines_b200.clifford import emitter_sample
+    from photonic_engines_b200.clifford.emitter import gap_terms
+    from photonic_engines_b200.states import caterpillar, spin_gate
+
+    n, m, shots = 12, 24, 512
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    st = caterpillar(n, [spin_gate(math.pi / 2, 0)] * n, m=m)
+    g = torch.Generator().manual_seed(n)
+    U_host = torch.linalg.qr(torch.randn(m, m, dtype=torch.complex128, generator=g))[0].contiguous()
+    U = U_host.to(dev)
+    peak = NAT.pipe_peak_tflops("f64", dev)
+    for i in range(args.warmup):
+        emitter_sample(st, U, shots, generator=torch.Generator().manual_seed(100 + i))
+    torch.cuda.synchronize()
+    kern_ms, flops = 0.0, 0.0
+    with ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        for i in range(args.steps):
+            _, stats = emitter_sample(st, U, shots, generator=torch.Generator().manual_seed(i), return_stats=True)
+            kern_ms += sum(stats["kernel_ms"])
+            flops += sum(stats["flops"])
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    # end to end: U from pinned host memory every step, occupations back to the host
+    U_pin = U_host.pin_memory()
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for i in range(args.steps):
+        occ = emitter_sample(st, U_pin.to(dev, non_blocking=True), shots, generator=torch.Generator().manual_seed(i))
+        occ.cpu()
+    e2e = args.steps * shots / (time.perf_counter() - t1)
+    # CPU baseline: per stream and step, the pure terms and the numpy matrix-cofactor sums (16 streams)
+    rng = np.random.default_rng(0)
+    Un = U_host.numpy()
+    t2 = time.perf_counter()
+    nb = 16
+    for _ in range(nb):
+        order = rng.permutation(n)
+        rows = []
+        for k in range(1, n + 1):
+            kept, s0, mats, f = gap_terms(st, order[:k].tolist(), torch.eye(2, dtype=torch.complex128)[0])
+            colmode = np.array([list(st.modes[j]) for j in kept])
+            w = EO.matrix_weights(Un, colmode, rows, s0.numpy(), mats.numpy(), f.numpy())
+            rows.append(int(rng.choice(m, p=w / w.sum())))
+    cpu = nb / (time.perf_counter() - t2)
+    ach = flops / (kern_ms * 1e-3) / 1e12
+    line = {"config": "emitter", "workload": f"EmitterMPS linear cluster (caterpillar), n={n} photons, m={m}, "
+                                              f"chi=2, 2 labels, emitter traced, {shots} shots/step, Haar U",
+            "metric": "samples/s", "unit": "samples/s", "value": args.steps * shots / dt,
+            "ms_per_step": dt / args.steps * 1e3, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "dtype": "f64", "data": "synthetic", "kernel_share": kern_ms * 1e-3 / dt,
+            "roofline": {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                         "traffic": None, "flops_per_step": flops / args.steps,
+                         "kernel_ms_per_step": kern_ms / args.steps},
+            "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": U_host.numel() * 16,
+                    "d2h_bytes_per_step": shots * m * 8},
+            "cpu_baseline": {"value": cpu, "unit": "samples/s", "cores": torch.get_num_threads(), "kind": "port",
+                             "sample": f"{nb} streams, host pure terms + numpy matrix-cofactor sums per step"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -458,7 +535,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--ref-shots", type=int, default=0, help="chains per CPU sample (0: scaled to the cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", choices=("c1", "c2", "c3", "c4", "c5"), default="c2",
+    ap.add_argument("--config", choices=("c1", "c2", "c3", "c4", "c5", "emitter"), default="c2",
                     help="c2 (default) is the headline line; the others print one line through the batched sampler")
     ap.add_argument("--profile-launch", choices=("f64", "mixed"), default=None,
                     help="run only two chain launches of the workload (a target for ncu -s 1 -c 1)")
@@ -468,6 +545,9 @@ def main():
         return
     if args.warmup < 3:
         args.warmup = 3
+    if args.config == "emitter" and args.impl == "b200":
+        run_emitter(args)
+        return
     if args.config != "c2" and args.impl == "b200":
         run_config(args)
         return

@@ -9,11 +9,12 @@ decomposed into orthogonal Kraus operators); output mode rho is drawn with weigh
 w(rho) = sum_e |amp_e(rho)|^2, amp_e(rho) = sum_c sum_l U[rho, mode(c, l)] Tr(M~_{e,c,l} K_{e,c}), the
 matrix cofactors K_{e,c} being Glynn sums over delta with chi x chi matrix chains.
 
-Here the term decomposition (small SVDs, cached per (T, final spin)) runs on the host as in the
-reference; the per-step sum over every (stream, term) lane and every sign vector runs in one launch of
-`pe_emitter_weights` (csrc/emitter.cu), and the draw consumes the caller's generator exactly as the
-reference's torch sampler does (final spin, photon order, one multinomial per step), so a seeded CPU
-generator gives the reference's samples.
+Here the pieces of the term decomposition (small SVDs: images of the initial and final emitter vectors,
+Kraus operators of every gap between placed photons) are computed once per call on the host and every
+stream's terms are assembled from them with batched device ops; the per-step sum over every (stream, term)
+lane and every sign vector runs in one launch of `pe_emitter_weights` (csrc/emitter.cu), and the draw
+consumes the caller's generator exactly as the reference's torch sampler does (final spin, photon order,
+one multinomial per step), so a seeded CPU generator gives the reference's samples.
 """
 from __future__ import annotations
 
@@ -122,8 +123,141 @@ class _Terms:
         return self.cache[key]
 
 
+class _Tables:
+    """The pieces every placed-photon set's pure terms are built from, for one state (and final spin):
+    the images of |s0> through the photons before the first placed one (PRE[a], a = first placed slot), the
+    images of <final| through the photons after the last placed one (SUF[fid, b]), and the Kraus operators
+    of every run of unplaced photons between placed slots a < b (GAP[a, b]; one identity for b = a + 1).
+    Each is built slot by slot with the SVD reduction of `gap_terms`, so the terms assembled from them are
+    those of `gap_terms` (same order, same values); O(n^2) small SVDs per state instead of some per set."""
+
+    def __init__(self, state: EmitterMPS, device):
+        n, chi = state.n, state.chi
+        ops = torch.as_tensor(state.ops, dtype=C128)
+        s0 = torch.as_tensor(state.s0, dtype=C128)
+        finals = [torch.as_tensor(state.final, dtype=C128)] if state.final is not None else \
+            list(torch.eye(chi, dtype=C128))
+        pre = [s0.unsqueeze(0)]
+        for a in range(1, n):
+            pre.append(_span_rows(torch.einsum("lts,rs->rlt", ops[a - 1], pre[-1]).reshape(-1, chi)))
+        suf = []
+        for f in finals:
+            row = [None] * n
+            W = f.conj().unsqueeze(0)
+            row[n - 1] = W
+            for b in range(n - 1, 0, -1):
+                W = _span_rows(torch.einsum("rs,lst->rlt", W, ops[b]).reshape(-1, chi))
+                row[b - 1] = W
+            suf.append([w.conj() for w in row])
+        gmax = chi * chi
+        GAP = torch.zeros(n, n, gmax, chi, chi, dtype=C128)
+        RG = torch.zeros(n, n, dtype=torch.int64)
+        for a in range(n - 1):
+            GAP[a, a + 1, 0] = torch.eye(chi, dtype=C128)
+            RG[a, a + 1] = 1
+            K = torch.eye(chi, dtype=C128).unsqueeze(0)
+            for b in range(a + 2, n):
+                K = _kraus(torch.einsum("lts,rsu->rltu", ops[b - 1], K).reshape(-1, chi, chi))
+                GAP[a, b, :K.shape[0]] = K
+                RG[a, b] = K.shape[0]
+        PRE = torch.zeros(n, chi, chi, dtype=C128)
+        R0 = torch.zeros(n, dtype=torch.int64)
+        for a, V in enumerate(pre):
+            PRE[a, :V.shape[0]] = V
+            R0[a] = V.shape[0]
+        SUF = torch.zeros(len(finals), n, chi, chi, dtype=C128)
+        RF = torch.zeros(len(finals), n, dtype=torch.int64)
+        for fi, row in enumerate(suf):
+            for b, W in enumerate(row):
+                SUF[fi, b, :W.shape[0]] = W
+                RF[fi, b] = W.shape[0]
+        self.ops = ops.to(device)
+        self.PRE, self.R0, self.SUF, self.RF = PRE.to(device), R0.to(device), SUF.to(device), RF.to(device)
+        self.GAP, self.RG = GAP.to(device), RG.to(device)
+
+    def lanes(self, T: torch.Tensor, fid: torch.Tensor):
+        """Every stream's pure terms for its placed slots T [S, k] (sorted, device) and final ids fid [S]:
+        (s0 [nl, chi], mats [nl, k, L, chi, chi], f [nl, chi], lstart [S], nlan [S]) with the lanes of a
+        stream contiguous and in gap_terms' order; zero-norm terms dropped by gap_terms' rule."""
+        S, k = T.shape
+        dev = T.device
+        r0 = self.R0[T[:, 0]]
+        rf = self.RF[fid, T[:, -1]]
+        rg = self.RG[T[:, :-1], T[:, 1:]] if k > 1 else torch.ones(S, 0, dtype=torch.int64, device=dev)
+        R = r0 * rf * rg.prod(dim=1)
+        nl = int(R.sum())
+        ls = torch.repeat_interleave(torch.arange(S, device=dev), R)
+        start = torch.cumsum(R, 0) - R
+        rem = torch.arange(nl, device=dev) - start[ls]
+        Tl = T[ls]
+        mats = self.ops[Tl]                                                   # [nl, k, L, chi, chi]
+        gsel = []
+        for j in range(k - 2, -1, -1):                                       # last gap is the fastest digit
+            rk = rg[ls, j]
+            gsel.append(rem % rk)
+            rem = rem // rk
+        gsel = gsel[::-1]
+        rfl = rf[ls]
+        i_f, i_0 = rem % rfl, rem // rfl
+        for j in range(k - 1):
+            K = self.GAP[Tl[:, j], Tl[:, j + 1], gsel[j]]                      # [nl, chi, chi]
+            mats[:, j] = torch.einsum("rts,rlsu->rltu", K, mats[:, j])
+        s0 = self.PRE[Tl[:, 0], i_0]
+        f = self.SUF[fid[ls], Tl[:, -1], i_f]
+        chi = s0.shape[1]
+        v = torch.einsum("rs,rt->rst", s0, s0.conj()).reshape(nl, chi * chi)
+        for j in range(k):
+            E = torch.einsum("rlts,rluv->rtusv", mats[:, j], mats[:, j].conj()).reshape(nl, chi * chi, chi * chi)
+            v = torch.einsum("rab,rb->ra", E, v)
+        fv = torch.einsum("rs,rt->rst", f, f.conj()).reshape(nl, chi * chi)
+        norm2 = torch.einsum("ra,ra->r", fv.conj(), v).real
+        scale = (f.abs() ** 2).sum(1) * (s0.abs() ** 2).sum(1)
+        keep = norm2 > 1e-14 * scale.clamp_min(1.0)
+        nlan = torch.zeros(S, dtype=torch.int64, device=dev).index_add_(0, ls, keep.to(torch.int64))
+        lstart = torch.cumsum(nlan, 0) - nlan
+        return s0[keep].contiguous(), mats[keep].contiguous(), f[keep].contiguous(), lstart, nlan
+
+
+def batched_step_weights(U_t: torch.Tensor, state: EmitterMPS, T: torch.Tensor, rows: torch.Tensor, fid: torch.Tensor,
+                         tables: _Tables, events: list | None = None) -> tuple[torch.Tensor, int]:
+    """(w [S, m] float64, lanes) of one step for every stream, everything on U's device: T [S, k] placed slots
+    (sorted), rows [S, >= k - 1] the chosen rows, fid [S] final ids.  Terms from `tables`, one launch of
+    pe_emitter_weights."""
+    dev = U_t.device
+    m = U_t.shape[0]
+    S, k = T.shape
+    s0, mats, f, lstart, nlan = tables.lanes(T, fid)
+    nl = int(s0.shape[0])
+    lane_stream = torch.repeat_interleave(torch.arange(S, device=dev), nlan)
+    lane_term = torch.arange(nl, device=dev)
+    modes = torch.tensor([list(mk) for mk in state.modes], dtype=torch.int32, device=dev)
+    colmode = modes[T].contiguous()
+    ut = torch.view_as_real(U_t.transpose(0, 1).contiguous()).contiguous()
+    amp = torch.empty(max(nl, 1), m, dtype=C128, device=dev)
+    w = torch.empty(S, m, dtype=torch.float64, device=dev)
+    ws = torch.empty(int(N.load().pe_emitter_workspace_bytes()), dtype=torch.uint8, device=dev)
+    rows_d = rows.contiguous()
+    if events is not None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+    rc = N.load().pe_emitter_weights(N.ptr(ut), m, int(U_t.shape[1]), N.ptr(rows_d), int(rows_d.shape[1]),
+                                     N.ptr(colmode), S, k, state.num_labels, state.chi, N.ptr(torch.view_as_real(s0)),
+                                     N.ptr(torch.view_as_real(f)), N.ptr(torch.view_as_real(mats)), nl,
+                                     N.ptr(lane_term), N.ptr(lane_stream), N.ptr(lstart), N.ptr(nlan), nl,
+                                     N.ptr(torch.view_as_real(amp)), N.ptr(w), N.ptr(ws), int(ws.numel()),
+                                     N.stream_handle(dev))
+    N.check(rc, "pe_emitter_weights")
+    if events is not None:
+        e1.record()
+        events.append((e0, e1, nl, k))
+    st, det = N.read_status(ws)
+    if st != 0:
+        raise N.NativeError(f"pe_emitter_weights: device-side index error at {det}")
+    return w, nl
+
+
 def step_weights(U_t: torch.Tensor, state: EmitterMPS, Tsorted: torch.Tensor, rows: torch.Tensor, fid: torch.Tensor,
-                 terms: _Terms, k: int) -> tuple[torch.Tensor, int]:
+                 terms: _Terms, k: int, events: list | None = None) -> tuple[torch.Tensor, int]:
     """(w [S, m] float64 on U's device, lanes) of step k for every stream: Tsorted [S, k] placed slots
     (sorted), rows [S, >= k - 1] the chosen rows (device), fid [S] final-spin ids.  One launch of
     pe_emitter_weights over all (stream, term) lanes."""
@@ -159,6 +293,9 @@ def step_weights(U_t: torch.Tensor, state: EmitterMPS, Tsorted: torch.Tensor, ro
     tensors = [t.to(dev).contiguous() for t in (colmode, lane_term, lane_stream, lstart, nlan)]
     colmode_d, lane_term_d, lane_stream_d, lstart_d, nlan_d = tensors
     rows_d = rows.to(dev, torch.int64).contiguous()
+    if events is not None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
     rc = N.load().pe_emitter_weights(N.ptr(ut), m, int(U_t.shape[1]), N.ptr(rows_d), int(rows_d.shape[1]),
                                      N.ptr(colmode_d), S, k, L, state.chi, N.ptr(torch.view_as_real(s0)),
                                      N.ptr(torch.view_as_real(f)), N.ptr(torch.view_as_real(mats)), int(s0.shape[0]),
@@ -166,6 +303,9 @@ def step_weights(U_t: torch.Tensor, state: EmitterMPS, Tsorted: torch.Tensor, ro
                                      N.ptr(torch.view_as_real(amp)), N.ptr(w), N.ptr(ws), int(ws.numel()),
                                      N.stream_handle(dev))
     N.check(rc, "pe_emitter_weights")
+    if events is not None:
+        e1.record()
+        events.append((e0, e1, nl, k))
     st, det = N.read_status(ws)
     if st != 0:
         raise N.NativeError(f"pe_emitter_weights: device-side index error at {det}")
@@ -209,11 +349,13 @@ def emitter_sample(state: EmitterMPS, U: torch.Tensor, shots: int, generator: to
     sigma = torch.argsort(torch.rand((S, n), generator=generator, device=gdev), dim=1).cpu()
     rows = torch.zeros((S, n), dtype=torch.long)
     rows_d = torch.zeros((S, max(n, 1)), dtype=torch.int64, device=dev)
-    terms = _Terms(state)
+    tables = _Tables(state, dev)
+    sigma_d, fid_d = sigma.to(dev), fid.to(dev)
     stats = {"R": []}                                                    # mean lanes (pure terms) per stream
+    events = [] if return_stats else None
     for k in range(1, n + 1):
-        Tsorted = torch.sort(sigma[:, :k], dim=1).values
-        w, nl = step_weights(U_t, state, Tsorted, rows_d, fid, terms, k)
+        Tsorted = torch.sort(sigma_d[:, :k], dim=1).values
+        w, nl = batched_step_weights(U_t, state, Tsorted, rows_d, fid_d, tables, events)
         w = w.cpu()
         w = w.clamp_min(0)
         w = w / w.sum(dim=1, keepdim=True)
@@ -224,7 +366,21 @@ def emitter_sample(state: EmitterMPS, U: torch.Tensor, shots: int, generator: to
     occ = torch.zeros((S, m), dtype=torch.long)
     occ.scatter_add_(1, rows, torch.ones_like(rows))
     occ = occ.to(dev)
+    if return_stats:
+        torch.cuda.synchronize(dev)
+        # kernel time per step and its work: lane-steps times the sign vectors and columns each one walks
+        stats["kernel_ms"] = [a.elapsed_time(b) for a, b, _, _ in events]
+        stats["flops"] = [emitter_step_flops(nl_, k_, state.num_labels) for _, _, nl_, k_ in events]
     return (occ, stats) if return_stats else occ
 
 
-__all__ = ["emitter_sample", "final_spin_distribution", "gap_terms", "step_weights"]
+def emitter_step_flops(lanes: int, k: int, L: int) -> float:
+    """Algorithmic FLOPs of one emitter step: lanes x 2^(k-2) sign vectors (1 when k <= 2) x k columns x
+    128 L (per column and label: the 2 x 2 products of the backward and forward chains, the trace and the
+    column-sum terms — 16 complex multiply-adds of 8 real FLOPs), plus the Gray update of the column sums."""
+    D = 2 ** (k - 2) if k >= 2 else 1
+    return float(lanes) * D * k * 128 * L
+
+
+__all__ = ["batched_step_weights", "emitter_sample", "emitter_step_flops", "final_spin_distribution", "gap_terms",
+           "step_weights"]

@@ -106,3 +106,32 @@ class EmitterMPS:
         """NotImplementedError for a chain whose events have different label counts."""
         if self.is_ragged:
             raise NotImplementedError(f"ragged label counts ({tuple(len(mk) for mk in self.modes)}): not in {where}")
+
+
+def spin_gate(theta: float, phi: float):
+    """Ry(theta/2) Rz(phi) Ry(theta/2) (2 x 2): the spin rotation between two emissions of a caterpillar
+    emitter (the reference's `spin_gate`, photonic_engines/states.py:850-861)."""
+    import numpy as np
+
+    def ry(t):
+        c, s = math.cos(t / 2), math.sin(t / 2)
+        return np.array([[c, -s], [s, c]], dtype=np.complex128)
+
+    rz = np.diag([np.exp(-0.5j * phi), np.exp(0.5j * phi)]).astype(np.complex128)
+    return ry(theta / 2) @ rz @ ry(theta / 2)
+
+
+def caterpillar(n: int, spin_gates, m: int | None = None, modes=None, s0=(1.0, 0.0), final=None) -> EmitterMPS:
+    """A spin emitting photon k into mode modes[k][0] when up and modes[k][1] when down, after the spin gate
+    spin_gates[k] (the reference's `EmitterMPS.caterpillar`, photonic_engines/states.py:455-483): ops[k, 0] =
+    P_up G_k, ops[k, 1] = P_down G_k; default modes (2k, 2k + 1) and m = 2n.  spin_gate(pi/2, 0) everywhere
+    gives the linear cluster state."""
+    import numpy as np
+    if len(spin_gates) != n:
+        raise ValueError("one spin gate per emission")
+    modes = [(2 * k, 2 * k + 1) for k in range(n)] if modes is None else modes
+    m = max(x for mk in modes for x in mk) + 1 if m is None else m
+    up, down = np.diag([1.0, 0.0]).astype(np.complex128), np.diag([0.0, 1.0]).astype(np.complex128)
+    ops = np.stack([np.stack([up @ np.asarray(G, dtype=np.complex128), down @ np.asarray(G, dtype=np.complex128)])
+                    for G in spin_gates])
+    return EmitterMPS(ops=ops, modes=tuple(tuple(mk) for mk in modes), s0=s0, m=m, final=final)

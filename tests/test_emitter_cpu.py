@@ -113,3 +113,25 @@ def test_emitter_sample_argument_checks():
         emitter_sample(EmitterMPS(ops=np.zeros((2, 1, 3, 3)), modes=((0,), (1,)), s0=[1, 0, 0], m=3), U[:3, :3], 2)
     with pytest.raises(ValueError):
         emitter_sample(st, U, 4, backend="nope")
+
+
+@pytest.mark.parametrize("final", [True, False])
+def test_batched_lanes_are_the_per_set_terms(final):
+    """The per-state tables assemble, for many placed-photon sets at once, exactly gap_terms' terms
+    (same lanes, same order, same values)."""
+    from photonic_engines_b200.clifford.emitter import _Tables
+    rng = np.random.default_rng(3 + final)
+    n = 7
+    ops = rng.normal(size=(n, 2, 2, 2)) + 1j * rng.normal(size=(n, 2, 2, 2))
+    st = EmitterMPS(ops=ops, modes=tuple(tuple(range(2 * k, 2 * k + 2)) for k in range(n)), s0=rng.normal(size=2),
+                    m=15, final=(rng.normal(size=2) + 1j * rng.normal(size=2)) if final else None)
+    tb = _Tables(st, "cpu")
+    for k in range(1, n + 1):
+        T = torch.tensor([sorted(rng.choice(n, size=k, replace=False).tolist()) for _ in range(6)])
+        fid = torch.as_tensor(rng.integers(0, 1 if final else 2, size=6))
+        s0, mats, f, lstart, nlan = tb.lanes(T, fid)
+        for s in range(6):
+            fv = None if final else torch.eye(2, dtype=torch.complex128)[int(fid[s])]
+            _, a0, am, af = gap_terms(st, T[s].tolist(), fv)
+            sl = slice(int(lstart[s]), int(lstart[s] + nlan[s]))
+            assert torch.equal(a0, s0[sl]) and torch.equal(am, mats[sl]) and torch.equal(af, f[sl]), (k, s)
