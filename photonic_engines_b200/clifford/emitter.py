@@ -218,11 +218,30 @@ class _Tables:
         return s0[keep].contiguous(), mats[keep].contiguous(), f[keep].contiguous(), lstart, nlan
 
 
+_TABLES: dict = {}
+
+
+def tables_for(state: EmitterMPS, device) -> _Tables:
+    """The state's tables on `device`, built on first use and kept while the state object lives (a state
+    is immutable, so its tables never change)."""
+    import weakref
+    key = (id(state), str(torch.device(device)))
+    hit = _TABLES.get(key)
+    if hit is not None and hit[0]() is state:
+        return hit[1]
+    tb = _Tables(state, device)
+    _TABLES[key] = (weakref.ref(state), tb)
+    weakref.finalize(state, _TABLES.pop, key, None)
+    return tb
+
+
 def batched_step_weights(U_t: torch.Tensor, state: EmitterMPS, T: torch.Tensor, rows: torch.Tensor, fid: torch.Tensor,
-                         tables: _Tables, events: list | None = None) -> tuple[torch.Tensor, int]:
+                         tables: _Tables, events: list | None = None, ws: torch.Tensor | None = None,
+                         ut: torch.Tensor | None = None) -> tuple[torch.Tensor, int]:
     """(w [S, m] float64, lanes) of one step for every stream, everything on U's device: T [S, k] placed slots
     (sorted), rows [S, >= k - 1] the chosen rows, fid [S] final ids.  Terms from `tables`, one launch of
-    pe_emitter_weights."""
+    pe_emitter_weights.  With `ws` (a workspace the caller checks later; pe_emitter_weights clears it, so
+    one per step) the device status is not read here."""
     dev = U_t.device
     m = U_t.shape[0]
     S, k = T.shape
@@ -232,10 +251,13 @@ def batched_step_weights(U_t: torch.Tensor, state: EmitterMPS, T: torch.Tensor, 
     lane_term = torch.arange(nl, device=dev)
     modes = torch.tensor([list(mk) for mk in state.modes], dtype=torch.int32, device=dev)
     colmode = modes[T].contiguous()
-    ut = torch.view_as_real(U_t.transpose(0, 1).contiguous()).contiguous()
+    if ut is None:
+        ut = torch.view_as_real(U_t.transpose(0, 1).contiguous()).contiguous()
     amp = torch.empty(max(nl, 1), m, dtype=C128, device=dev)
     w = torch.empty(S, m, dtype=torch.float64, device=dev)
-    ws = torch.empty(int(N.load().pe_emitter_workspace_bytes()), dtype=torch.uint8, device=dev)
+    own_ws = ws is None
+    if own_ws:
+        ws = torch.empty(int(N.load().pe_emitter_workspace_bytes()), dtype=torch.uint8, device=dev)
     rows_d = rows.contiguous()
     if events is not None:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -250,9 +272,10 @@ def batched_step_weights(U_t: torch.Tensor, state: EmitterMPS, T: torch.Tensor, 
     if events is not None:
         e1.record()
         events.append((e0, e1, nl, k))
-    st, det = N.read_status(ws)
-    if st != 0:
-        raise N.NativeError(f"pe_emitter_weights: device-side index error at {det}")
+    if own_ws:
+        st, det = N.read_status(ws)
+        if st != 0:
+            raise N.NativeError(f"pe_emitter_weights: device-side index error at {det}")
     return w, nl
 
 
@@ -349,13 +372,16 @@ def emitter_sample(state: EmitterMPS, U: torch.Tensor, shots: int, generator: to
     sigma = torch.argsort(torch.rand((S, n), generator=generator, device=gdev), dim=1).cpu()
     rows = torch.zeros((S, n), dtype=torch.long)
     rows_d = torch.zeros((S, max(n, 1)), dtype=torch.int64, device=dev)
-    tables = _Tables(state, dev)
+    tables = tables_for(state, dev)
     sigma_d, fid_d = sigma.to(dev), fid.to(dev)
+    ut = torch.view_as_real(U_t.transpose(0, 1).contiguous()).contiguous()
+    wsb = int(N.load().pe_emitter_workspace_bytes())
+    wss = torch.empty(n, wsb, dtype=torch.uint8, device=dev)           # one status word per step, read once
     stats = {"R": []}                                                    # mean lanes (pure terms) per stream
     events = [] if return_stats else None
     for k in range(1, n + 1):
         Tsorted = torch.sort(sigma_d[:, :k], dim=1).values
-        w, nl = batched_step_weights(U_t, state, Tsorted, rows_d, fid_d, tables, events)
+        w, nl = batched_step_weights(U_t, state, Tsorted, rows_d, fid_d, tables, events, wss[k - 1], ut)
         w = w.cpu()
         w = w.clamp_min(0)
         w = w / w.sum(dim=1, keepdim=True)
@@ -363,6 +389,11 @@ def emitter_sample(state: EmitterMPS, U: torch.Tensor, shots: int, generator: to
         rows[:, k - 1] = rho
         rows_d[:, k - 1] = rho.to(dev)
         stats["R"].append(nl / max(S, 1))
+    status = wss[:, 8:12].contiguous().cpu().view(torch.int32).reshape(-1)     # the status word of every step
+    if bool((status != 0).any()):
+        k_bad = int(torch.nonzero(status)[0, 0])
+        _, det = N.read_status(wss[k_bad])
+        raise N.NativeError(f"pe_emitter_weights: device-side index error at step {k_bad + 1}, lane {det}")
     occ = torch.zeros((S, m), dtype=torch.long)
     occ.scatter_add_(1, rows, torch.ones_like(rows))
     occ = occ.to(dev)

@@ -8,7 +8,8 @@
 // then amp(rho) = 2^-(k-2) sum_c sum_l U[rho, mode(c, l)] t_{c,l} for every output mode rho, and the
 // stream's weight w(rho) = sum over its lanes of |amp(rho)|^2.  This is the reference's
 // matrix_cofactor_weights (photonic_engines/clifford/emitter_reference.py:280-305) and the step of
-// emitter_sampler.sample_torch (emitter_sampler.py:150-175), restated for one CTA per lane.
+// emitter_sampler.sample_torch (emitter_sampler.py:150-175), restated for one warp per lane (k <= 8) or
+// one CTA per lane (longer chains, whose 2^(k-2) sign vectors are spread over the CTA's threads).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -49,6 +50,95 @@ static __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 }
 static __device__ __forceinline__ double2 cmac(double2 acc, double2 a, double2 b) {   // acc + a b
     return make_double2(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));
+}
+
+
+// The Gray-ordered walk over sign-vector indices [t0, t1) of one lane: column sums, backward chain
+// (stored), forward chain and the trace accumulators acc[c][l] += sign * q_c M_{c,l} p_c.  M and the
+// rows' U entries are read from shared memory (sM[c][l][a][b], sU[i][j][l]).
+template <int KE, int NL>
+__device__ __forceinline__ void walk(const double2 (*sM)[NL][CHI][CHI], const double2 (*sU)[KE][NL], int k,
+                                     int64_t t0, int64_t t1, double2 s00, double2 s01, double2 fc0, double2 fc1,
+                                     double2 (&acc)[KE][NL]) {
+    const int kk = k - 1;
+#pragma unroll
+    for (int j = 0; j < KE; ++j)
+#pragma unroll
+        for (int l = 0; l < NL; ++l) acc[j][l] = make_double2(0.0, 0.0);
+    if (t0 < t1) {
+        double2 cs[KE][NL];
+        uint64_t g = (uint64_t)(t0 ^ (t0 >> 1));
+#pragma unroll
+        for (int j = 0; j < KE; ++j)
+#pragma unroll
+            for (int l = 0; l < NL; ++l) {
+                double2 x = make_double2(kk == 0 ? 1.0 : 0.0, 0.0);
+                if (j < k) {
+                    for (int i = 0; i < kk; ++i) {
+                        const double d = (i == 0 || !((g >> (i - 1)) & 1)) ? 1.0 : -1.0;
+                        x.x = fma(d, sU[i][j][l].x, x.x);
+                        x.y = fma(d, sU[i][j][l].y, x.y);
+                    }
+                }
+                cs[j][l] = x;
+            }
+        double sign = (__popcll(g) & 1) ? -1.0 : 1.0;
+        for (int64_t t = t0; t < t1; ++t) {
+            if (t > t0) {                                   // Gray step into t: free bit b flips
+                const int b = __ffsll((long long)t) - 1;
+                g ^= (uint64_t)1 << b;
+                const double d2 = ((g >> b) & 1) ? -2.0 : 2.0;   // 2 * new delta of row b + 1
+                const int i = b + 1;
+#pragma unroll
+                for (int j = 0; j < KE; ++j)
+#pragma unroll
+                    for (int l = 0; l < NL; ++l)
+                        if (j < k) {
+                            cs[j][l].x = fma(d2, sU[i][j][l].x, cs[j][l].x);
+                            cs[j][l].y = fma(d2, sU[i][j][l].y, cs[j][l].y);
+                        }
+                sign = -sign;
+            }
+            // backward: q_c (stored), u <- u G_c
+            double2 q0[KE], q1[KE];
+            double2 u0 = fc0, u1 = fc1;
+#pragma unroll
+            for (int c = KE - 1; c >= 0; --c) {
+                if (c < k) {
+                    q0[c] = u0; q1[c] = u1;
+                    double2 n0 = make_double2(0.0, 0.0), n1 = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int l = 0; l < NL; ++l) {
+                        // z = u M_{c,l} (row vector), then u' += colsum z
+                        const double2 z0 = cmac(cmul(u0, sM[c][l][0][0]), u1, sM[c][l][1][0]);
+                        const double2 z1 = cmac(cmul(u0, sM[c][l][0][1]), u1, sM[c][l][1][1]);
+                        n0 = cmac(n0, cs[c][l], z0);
+                        n1 = cmac(n1, cs[c][l], z1);
+                    }
+                    u0 = n0; u1 = n1;
+                }
+            }
+            // forward: y = M_{c,l} v, t_{c,l} += sign q_c . y, v <- sum_l colsum y
+            double2 v0 = s00, v1 = s01;
+#pragma unroll
+            for (int c = 0; c < KE; ++c) {
+                if (c < k) {
+                    double2 n0 = make_double2(0.0, 0.0), n1 = make_double2(0.0, 0.0);
+#pragma unroll
+                    for (int l = 0; l < NL; ++l) {
+                        const double2 y0 = cmac(cmul(sM[c][l][0][0], v0), sM[c][l][0][1], v1);
+                        const double2 y1 = cmac(cmul(sM[c][l][1][0], v0), sM[c][l][1][1], v1);
+                        const double2 dt = cmac(cmul(q0[c], y0), q1[c], y1);
+                        acc[c][l].x = fma(sign, dt.x, acc[c][l].x);
+                        acc[c][l].y = fma(sign, dt.y, acc[c][l].y);
+                        n0 = cmac(n0, cs[c][l], y0);
+                        n1 = cmac(n1, cs[c][l], y1);
+                    }
+                    v0 = n0; v1 = n1;
+                }
+            }
+        }
+    }
 }
 
 template <int KE, int NL>
@@ -109,84 +199,7 @@ __global__ void __launch_bounds__(THREADS) emitter_amp_kernel(Params p) {
         if (D >= THREADS) { const int64_t per = D / THREADS; t0 = tid * per; t1 = t0 + per; }
         else { t0 = tid; t1 = tid < D ? tid + 1 : tid; }
         double2 acc[KE][NL];
-#pragma unroll
-        for (int j = 0; j < KE; ++j)
-#pragma unroll
-            for (int l = 0; l < NL; ++l) acc[j][l] = make_double2(0.0, 0.0);
-        if (t0 < t1) {
-            double2 cs[KE][NL];
-            uint64_t g = (uint64_t)(t0 ^ (t0 >> 1));
-#pragma unroll
-            for (int j = 0; j < KE; ++j)
-#pragma unroll
-                for (int l = 0; l < NL; ++l) {
-                    double2 x = make_double2(kk == 0 ? 1.0 : 0.0, 0.0);
-                    if (j < k) {
-                        for (int i = 0; i < kk; ++i) {
-                            const double d = (i == 0 || !((g >> (i - 1)) & 1)) ? 1.0 : -1.0;
-                            x.x = fma(d, sU[i][j][l].x, x.x);
-                            x.y = fma(d, sU[i][j][l].y, x.y);
-                        }
-                    }
-                    cs[j][l] = x;
-                }
-            double sign = (__popcll(g) & 1) ? -1.0 : 1.0;
-            for (int64_t t = t0; t < t1; ++t) {
-                if (t > t0) {                                   // Gray step into t: free bit b flips
-                    const int b = __ffsll((long long)t) - 1;
-                    g ^= (uint64_t)1 << b;
-                    const double d2 = ((g >> b) & 1) ? -2.0 : 2.0;   // 2 * new delta of row b + 1
-                    const int i = b + 1;
-#pragma unroll
-                    for (int j = 0; j < KE; ++j)
-#pragma unroll
-                        for (int l = 0; l < NL; ++l)
-                            if (j < k) {
-                                cs[j][l].x = fma(d2, sU[i][j][l].x, cs[j][l].x);
-                                cs[j][l].y = fma(d2, sU[i][j][l].y, cs[j][l].y);
-                            }
-                    sign = -sign;
-                }
-                // backward: q_c (stored), u <- u G_c
-                double2 q0[KE], q1[KE];
-                double2 u0 = fc0, u1 = fc1;
-#pragma unroll
-                for (int c = KE - 1; c >= 0; --c) {
-                    if (c < k) {
-                        q0[c] = u0; q1[c] = u1;
-                        double2 n0 = make_double2(0.0, 0.0), n1 = make_double2(0.0, 0.0);
-#pragma unroll
-                        for (int l = 0; l < NL; ++l) {
-                            // z = u M_{c,l} (row vector), then u' += colsum z
-                            const double2 z0 = cmac(cmul(u0, sM[c][l][0][0]), u1, sM[c][l][1][0]);
-                            const double2 z1 = cmac(cmul(u0, sM[c][l][0][1]), u1, sM[c][l][1][1]);
-                            n0 = cmac(n0, cs[c][l], z0);
-                            n1 = cmac(n1, cs[c][l], z1);
-                        }
-                        u0 = n0; u1 = n1;
-                    }
-                }
-                // forward: y = M_{c,l} v, t_{c,l} += sign q_c . y, v <- sum_l colsum y
-                double2 v0 = s00, v1 = s01;
-#pragma unroll
-                for (int c = 0; c < KE; ++c) {
-                    if (c < k) {
-                        double2 n0 = make_double2(0.0, 0.0), n1 = make_double2(0.0, 0.0);
-#pragma unroll
-                        for (int l = 0; l < NL; ++l) {
-                            const double2 y0 = cmac(cmul(sM[c][l][0][0], v0), sM[c][l][0][1], v1);
-                            const double2 y1 = cmac(cmul(sM[c][l][1][0], v0), sM[c][l][1][1], v1);
-                            const double2 dt = cmac(cmul(q0[c], y0), q1[c], y1);
-                            acc[c][l].x = fma(sign, dt.x, acc[c][l].x);
-                            acc[c][l].y = fma(sign, dt.y, acc[c][l].y);
-                            n0 = cmac(n0, cs[c][l], y0);
-                            n1 = cmac(n1, cs[c][l], y1);
-                        }
-                        v0 = n0; v1 = n1;
-                    }
-                }
-            }
-        }
+        walk<KE, NL>(sM, sU, k, t0, t1, s00, s01, fc0, fc1, acc);
         // deterministic reduction: warp butterflies, then the warps in order
 #pragma unroll
         for (int j = 0; j < KE; ++j)
@@ -218,6 +231,99 @@ __global__ void __launch_bounds__(THREADS) emitter_amp_kernel(Params p) {
         }
         __syncthreads();
     }
+}
+
+// Short chains (k <= 8: at most 64 sign vectors per lane): one warp per lane, eight lanes per CTA, each
+// warp with its own slice of shared memory; no CTA barrier.
+constexpr int WW = 8;
+template <int NL>
+__global__ void __launch_bounds__(32 * WW) emitter_amp_warp_kernel(Params p) {
+    constexpr int KE = 8;
+    __shared__ double2 wM[WW][KE][NL][CHI][CHI];
+    __shared__ double2 wU[WW][KE][KE][NL];
+    __shared__ double2 wT[WW][KE][NL];
+    __shared__ int wMode[WW][KE][NL];
+    __shared__ int wRow[WW][KE];
+    const int lid = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int k = p.k, kk = k - 1;
+    for (int64_t lane = (int64_t)blockIdx.x * WW + wid; lane < p.nl; lane += (int64_t)gridDim.x * WW) {
+        const int64_t s = p.lane_stream[lane], e = p.lane_term[lane];
+        const bool bad_lane = s < 0 || s >= p.S || e < 0 || e >= p.Tt;
+        bool bad = false;
+        if (!bad_lane && lid < k * NL) {
+            const int j = lid / NL, l = lid % NL;
+            const int md = p.colmode[(s * k + j) * p.L + l];
+            if (md < 0 || md >= p.M) bad = true;
+            else wMode[wid][j][l] = md;
+        }
+        if (!bad_lane && lid < kk) {
+            const int64_t r = p.rows[s * p.rows_stride + lid];
+            if (r < 0 || r >= p.m) bad = true;
+            else wRow[wid][lid] = (int)r;
+        }
+        if (bad_lane || __any_sync(0xffffffffu, bad)) {
+            if (lid == 0) record(p.status, p.detail, lane);
+            __syncwarp();
+            continue;
+        }
+        for (int idx = lid; idx < k * NL * CHI * CHI; idx += 32) {
+            const int j = idx / (NL * CHI * CHI), rem = idx % (NL * CHI * CHI);
+            const int l = rem / (CHI * CHI), ab = rem % (CHI * CHI);
+            wM[wid][j][l][ab / CHI][ab % CHI] = p.mats[(e * k + j) * (int64_t)p.L * CHI * CHI + l * CHI * CHI + ab];
+        }
+        __syncwarp();
+        for (int idx = lid; idx < kk * k * NL; idx += 32) {
+            const int i = idx / (k * NL), rem = idx % (k * NL);
+            const int j = rem / NL, l = rem % NL;
+            wU[wid][i][j][l] = p.UT[(int64_t)wMode[wid][j][l] * p.m + wRow[wid][i]];
+        }
+        __syncwarp();
+        const double2 s00 = p.s0[e * CHI], s01 = p.s0[e * CHI + 1];
+        const double2 f0 = p.f[e * CHI], f1 = p.f[e * CHI + 1];
+        const int64_t D = kk >= 1 ? ((int64_t)1 << (kk - 1)) : 1;
+        int64_t t0, t1;
+        if (D >= 32) { const int64_t per = D / 32; t0 = lid * per; t1 = t0 + per; }
+        else { t0 = lid; t1 = lid < D ? lid + 1 : lid; }
+        double2 acc[KE][NL];
+        walk<KE, NL>(wM[wid], wU[wid], k, t0, t1, s00, s01, make_double2(f0.x, -f0.y), make_double2(f1.x, -f1.y), acc);
+        const double norm = kk >= 1 ? ldexp(1.0, -(kk - 1)) : 1.0;
+#pragma unroll
+        for (int j = 0; j < KE; ++j)
+#pragma unroll
+            for (int l = 0; l < NL; ++l) {
+                double2 x = acc[j][l];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    x.x += __shfl_xor_sync(0xffffffffu, x.x, o);
+                    x.y += __shfl_xor_sync(0xffffffffu, x.y, o);
+                }
+                if (lid == 0 && j < k) wT[wid][j][l] = make_double2(x.x * norm, x.y * norm);
+            }
+        __syncwarp();
+        for (int rho = lid; rho < p.m; rho += 32) {
+            double2 a = make_double2(0.0, 0.0);
+            for (int c = 0; c < k; ++c)
+#pragma unroll
+                for (int l = 0; l < NL; ++l) a = cmac(a, p.UT[(int64_t)wMode[wid][c][l] * p.m + rho], wT[wid][c][l]);
+            p.amp[lane * p.m + rho] = a;
+        }
+        __syncwarp();
+    }
+}
+
+template <int NL>
+static int launch_amp_warp(const Params& p, cudaStream_t st) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emitter_amp_warp_kernel<NL>, 32 * WW, 0) != cudaSuccess)
+        return PE_ERR_CUDA;
+    if (per < 1) return PE_ERR_SIZE;
+    int64_t grid = (int64_t)sms * per;
+    const int64_t need = (p.nl + WW - 1) / WW;
+    if (grid > need) grid = need;
+    emitter_amp_warp_kernel<NL><<<(unsigned)grid, 32 * WW, 0, st>>>(p);
+    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
 }
 
 // w[s][rho] = sum over the stream's lanes lstart[s] .. lstart[s] + nlan[s] - 1, in order, of |amp|^2.
@@ -287,7 +393,7 @@ extern "C" int pe_emitter_weights(const double* d_ut, int m, int M, const int64_
     p.detail = (long long*)((char*)d_workspace + 16);
     int rc = PE_OK;
     if (nl > 0) {
-        if (k <= 8) rc = L == 1 ? launch_amp<8, 1>(p, st) : launch_amp<8, 2>(p, st);
+        if (k <= 8) rc = L == 1 ? launch_amp_warp<1>(p, st) : launch_amp_warp<2>(p, st);
         else if (k <= 16) rc = L == 1 ? launch_amp<16, 1>(p, st) : launch_amp<16, 2>(p, st);
         else rc = L == 1 ? launch_amp<24, 1>(p, st) : launch_amp<24, 2>(p, st);
         if (rc != PE_OK) return rc;
