@@ -168,6 +168,30 @@ int pe_emitter_weights(const double* d_ut, int m, int M, const int64_t* d_rows, 
 size_t pe_emitter_workspace_bytes(void);
 
 /*
+ * The same emitter step with every term assembled on the device (no per-lane inputs): per-state tables
+ *   d_gops [n][n][4][L][2][2]  K^(a,b)_r M_{a,l}: Kraus operator r of the run of photons between placed
+ *                              slots a < b, times slot a's emission operator l;  d_rg [n][n] int32 ranks
+ *   d_ops  [n][L][2][2]        emission operators (the last placed slot)
+ *   d_pre  [n][2][2]           images of |s0> through the photons before slot a; d_r0 [n] int32 ranks
+ *   d_suf  [nf][n][2][2]       images of <final| through the photons after slot b; d_rf [nf][n] ranks
+ * (emitter_reference.py:190-277, gap_kraus_terms, split into its per-slot pieces), the streams' placed
+ * slots d_T [S][k] (increasing) and final ids d_fid [S], d_modes [n][L].  pe_emitter_count writes the
+ * number of terms of every stream (d_nlan [S]); the caller forms d_lstart = exclusive cumsum and nl, then
+ * pe_emitter_step writes d_amp [nl][m] and d_w [S][m] as pe_emitter_weights.  Terms whose norm is below
+ * 1e-14 of their scale add nothing (the reference drops them).  pe_emitter_count clears the workspace's
+ * status word, pe_emitter_step keeps it.
+ */
+int pe_emitter_count(const int32_t* d_T, const int32_t* d_fid, int64_t S, int k, const int32_t* d_rg,
+                     const int32_t* d_r0, const int32_t* d_rf, int n, int nf, int64_t* d_nlan, void* d_workspace,
+                     size_t workspace_bytes, void* stream);
+int pe_emitter_step(const double* d_ut, int m, int M, const int64_t* d_rows, int rows_stride, const int32_t* d_T,
+                    const int32_t* d_fid, const int32_t* d_modes, int64_t S, int k, int L, int chi,
+                    const double* d_gops, const int32_t* d_rg, const double* d_ops, const double* d_pre,
+                    const int32_t* d_r0, const double* d_suf, const int32_t* d_rf, int n, int nf,
+                    const int64_t* d_lstart, const int64_t* d_nlan, int64_t nl, double* d_amp, double* d_w,
+                    void* d_workspace, size_t workspace_bytes, void* stream);
+
+/*
  * pe_fock_chain without a workspace argument: the same chains and outputs, for callers that cannot
  * allocate device memory when they sample (a host callback or other context where CUDA allocation is not
  * allowed, a serving process whose device memory all belongs to its own arena, a foreign-language

@@ -71,6 +71,12 @@ def load() -> ctypes.CDLL:
                                      _vp, _vp, _vp, _i64, _vp, _vp, _vp, ctypes.c_size_t, _vp]
     L.pe_emitter_workspace_bytes.restype = ctypes.c_size_t
     L.pe_emitter_workspace_bytes.argtypes = []
+    L.pe_emitter_count.restype = _i32
+    L.pe_emitter_count.argtypes = [_vp, _vp, _i64, _i32, _vp, _vp, _vp, _i32, _i32, _vp, _vp, ctypes.c_size_t, _vp]
+    L.pe_emitter_step.restype = _i32
+    L.pe_emitter_step.argtypes = [_vp, _i32, _i32, _vp, _i32, _vp, _vp, _vp, _i64, _i32, _i32, _i32, _vp, _vp, _vp,
+                                  _vp, _vp, _vp, _vp, _i32, _i32, _vp, _vp, _i64, _vp, _vp, _vp, ctypes.c_size_t,
+                                  _vp]
     L.pe_fock_chain_noalloc.restype = _i32
     L.pe_fock_chain_noalloc.argtypes = [_i32, _vp, _vp, _vp, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i32, _vp, _vp, _vp,
                                         _vp, _vp, _vp, _vp, _i32, _vp, _i32, _vp, _i32, _i32, _i32, _vp]
@@ -94,7 +100,7 @@ def load() -> ctypes.CDLL:
 EXPORTED = ("pe_version", "pe_max_modes", "pe_chain_workspace_bytes", "pe_fock_chain", "pe_fock_chain_noalloc",
             "pe_fock_chain_split", "pe_chain_split_workspace_bytes", "pe_fock_chain_warp",
             "pe_fock_chain_adaptive", "pe_adaptive_workspace_bytes", "pe_emitter_weights",
-            "pe_emitter_workspace_bytes",
+            "pe_emitter_workspace_bytes", "pe_emitter_count", "pe_emitter_step",
             "pe_cofactors_rows", "pe_partition_shots", "pe_scatter_occupations", "pe_pipe_probe", "pe_read_status",
             "pe_status_string")
 

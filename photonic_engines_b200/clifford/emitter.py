@@ -10,9 +10,9 @@ w(rho) = sum_e |amp_e(rho)|^2, amp_e(rho) = sum_c sum_l U[rho, mode(c, l)] Tr(M~
 matrix cofactors K_{e,c} being Glynn sums over delta with chi x chi matrix chains.
 
 Here the pieces of the term decomposition (small SVDs: images of the initial and final emitter vectors,
-Kraus operators of every gap between placed photons) are computed once per call on the host and every
-stream's terms are assembled from them with batched device ops; the per-step sum over every (stream, term)
-lane and every sign vector runs in one launch of `pe_emitter_weights` (csrc/emitter.cu), and the draw
+Kraus operators of every gap between placed photons) are computed once per state on the host; per step,
+`pe_emitter_count` gives every stream's number of terms and `pe_emitter_step` (csrc/emitter.cu) assembles
+each (stream, term) lane from those tables on the device and sums it over every sign vector, and the draw
 consumes the caller's generator exactly as the reference's torch sampler does (final spin, photon order,
 one multinomial per step), so a seeded CPU generator gives the reference's samples.
 """
@@ -171,9 +171,15 @@ class _Tables:
             for b, W in enumerate(row):
                 SUF[fi, b, :W.shape[0]] = W
                 RF[fi, b] = W.shape[0]
+        # gap operator r after placed slot a (next placed slot b) times slot a's emission operators
+        GOPS = torch.einsum("abrts,alsu->abrltu", GAP, ops)                     # [n, n, 4, L, chi, chi]
         self.ops = ops.to(device)
         self.PRE, self.R0, self.SUF, self.RF = PRE.to(device), R0.to(device), SUF.to(device), RF.to(device)
         self.GAP, self.RG = GAP.to(device), RG.to(device)
+        self.GOPS = GOPS.contiguous().to(device)
+        self.rg32, self.r032, self.rf32 = (x.to(device, torch.int32).contiguous() for x in (RG, R0, RF))
+        self.modes32 = torch.tensor([list(mk) for mk in state.modes], dtype=torch.int32, device=device)
+        self.n, self.nf = n, len(finals)
 
     def lanes(self, T: torch.Tensor, fid: torch.Tensor):
         """Every stream's pure terms for its placed slots T [S, k] (sorted, device) and final ids fid [S]:
@@ -279,6 +285,42 @@ def batched_step_weights(U_t: torch.Tensor, state: EmitterMPS, T: torch.Tensor, 
     return w, nl
 
 
+def fused_step_weights(ut: torch.Tensor, m: int, state: EmitterMPS, T: torch.Tensor, rows: torch.Tensor,
+                       fid32: torch.Tensor, tables: _Tables, ws: torch.Tensor, events: list | None = None
+                       ) -> tuple[torch.Tensor, int]:
+    """(w [S, m] float64, lanes) of one step with the terms assembled on the device from `tables`:
+    pe_emitter_count (terms per stream), a cumsum for the lane offsets, pe_emitter_step.  T [S, k] int32
+    placed slots (sorted), rows [S, >= k - 1] int64, fid32 [S] int32, ut the [M][m] transposed U (real view),
+    ws a 256-byte workspace whose status word the caller reads."""
+    L_ = N.load()
+    dev = T.device
+    S, k = T.shape
+    st = N.stream_handle(dev)
+    nlan = torch.empty(S, dtype=torch.int64, device=dev)
+    N.check(L_.pe_emitter_count(N.ptr(T), N.ptr(fid32), S, k, N.ptr(tables.rg32), N.ptr(tables.r032),
+                                N.ptr(tables.rf32), tables.n, tables.nf, N.ptr(nlan), N.ptr(ws), int(ws.numel()), st),
+            "pe_emitter_count")
+    lstart = torch.cumsum(nlan, 0) - nlan
+    nl = int(nlan.sum())
+    amp = torch.empty(max(nl, 1), m, dtype=C128, device=dev)
+    w = torch.empty(S, m, dtype=torch.float64, device=dev)
+    if events is not None:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+    rc = L_.pe_emitter_step(N.ptr(ut), m, int(ut.shape[0]), N.ptr(rows), int(rows.shape[1]), N.ptr(T), N.ptr(fid32),
+                            N.ptr(tables.modes32), S, k, state.num_labels, state.chi,
+                            N.ptr(torch.view_as_real(tables.GOPS)), N.ptr(tables.rg32),
+                            N.ptr(torch.view_as_real(tables.ops)), N.ptr(torch.view_as_real(tables.PRE)),
+                            N.ptr(tables.r032), N.ptr(torch.view_as_real(tables.SUF)), N.ptr(tables.rf32), tables.n,
+                            tables.nf, N.ptr(lstart), N.ptr(nlan), nl, N.ptr(torch.view_as_real(amp)), N.ptr(w),
+                            N.ptr(ws), int(ws.numel()), st)
+    N.check(rc, "pe_emitter_step")
+    if events is not None:
+        e1.record()
+        events.append((e0, e1, nl, k))
+    return w, nl
+
+
 def step_weights(U_t: torch.Tensor, state: EmitterMPS, Tsorted: torch.Tensor, rows: torch.Tensor, fid: torch.Tensor,
                  terms: _Terms, k: int, events: list | None = None) -> tuple[torch.Tensor, int]:
     """(w [S, m] float64 on U's device, lanes) of step k for every stream: Tsorted [S, k] placed slots
@@ -373,15 +415,15 @@ def emitter_sample(state: EmitterMPS, U: torch.Tensor, shots: int, generator: to
     rows = torch.zeros((S, n), dtype=torch.long)
     rows_d = torch.zeros((S, max(n, 1)), dtype=torch.int64, device=dev)
     tables = tables_for(state, dev)
-    sigma_d, fid_d = sigma.to(dev), fid.to(dev)
+    sigma_d, fid32 = sigma.to(dev), fid.to(dev, torch.int32)
     ut = torch.view_as_real(U_t.transpose(0, 1).contiguous()).contiguous()
     wsb = int(N.load().pe_emitter_workspace_bytes())
     wss = torch.empty(n, wsb, dtype=torch.uint8, device=dev)           # one status word per step, read once
     stats = {"R": []}                                                    # mean lanes (pure terms) per stream
     events = [] if return_stats else None
     for k in range(1, n + 1):
-        Tsorted = torch.sort(sigma_d[:, :k], dim=1).values
-        w, nl = batched_step_weights(U_t, state, Tsorted, rows_d, fid_d, tables, events, wss[k - 1], ut)
+        Tsorted = torch.sort(sigma_d[:, :k], dim=1).values.to(torch.int32)
+        w, nl = fused_step_weights(ut, m, state, Tsorted, rows_d, fid32, tables, wss[k - 1], events)
         w = w.cpu()
         w = w.clamp_min(0)
         w = w / w.sum(dim=1, keepdim=True)
@@ -413,5 +455,5 @@ def emitter_step_flops(lanes: int, k: int, L: int) -> float:
     return float(lanes) * D * k * 128 * L
 
 
-__all__ = ["batched_step_weights", "emitter_sample", "emitter_step_flops", "final_spin_distribution", "gap_terms",
+__all__ = ["batched_step_weights", "emitter_sample", "fused_step_weights", "emitter_step_flops", "final_spin_distribution", "gap_terms",
            "step_weights"]

@@ -311,6 +311,288 @@ __global__ void __launch_bounds__(32 * WW) emitter_amp_warp_kernel(Params p) {
     }
 }
 
+// ---------------------------------------------------------------------------------------- fused step
+// The same step with every term assembled on the device from the per-state tables: a lane is (stream s,
+// term e < nlan[s]); its matrices are gathers of gops[a][b][r][l] = K^{(a,b)}_r M_{a,l} (the gap channel
+// after placed slot a, Kraus operator r, times the slot's emission operator) and of ops for the last
+// placed slot, its vectors rows of pre[a] (images of |s0>) and suf[fid][b] (images of <final|).  The term
+// index decodes as (i0, if, g_0 .. g_{k-2}) with g_{k-2} fastest; a term whose norm is below 1e-14 of its
+// scale contributes nothing (the rule of the host decomposition).
+struct Tables {
+    const double2* gops;     // [n][n][4][L][2][2]
+    const int32_t* rg;       // [n][n]
+    const double2* ops;      // [n][L][2][2]
+    const double2* pre;      // [n][2][2]
+    const int32_t* r0;       // [n]
+    const double2* suf;      // [nf][n][2][2]
+    const int32_t* rf;       // [nf][n]
+    int n, nf;
+};
+
+struct StepParams {
+    const double2* UT;
+    int m, M;
+    const int64_t* rows;
+    int rows_stride;
+    const int32_t* T;        // [S][k] placed slots, increasing
+    const int32_t* fid;      // [S]
+    const int32_t* modes;    // [n][L]
+    int64_t S;
+    int k, L;
+    Tables tb;
+    const int64_t* lstart;   // [S]
+    const int64_t* nlan;     // [S]
+    int64_t nl;
+    double2* amp;            // [nl][m]
+    int* status;
+    long long* detail;
+};
+
+// nlan[s] = number of terms of stream s (0 and an error record for invalid slots / final ids).
+__global__ void emitter_count_kernel(StepParams p, int64_t* nlan) {
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= p.S) return;
+    const int32_t* T = p.T + s * p.k;
+    const int fid = p.fid[s];
+    bool ok = fid >= 0 && fid < p.tb.nf;
+    int64_t R = 0;
+    if (ok) {
+        for (int j = 0; j < p.k; ++j) ok = ok && T[j] >= 0 && T[j] < p.tb.n && (j == 0 || T[j] > T[j - 1]);
+    }
+    if (ok) {
+        R = (int64_t)p.tb.r0[T[0]] * p.tb.rf[fid * p.tb.n + T[p.k - 1]];
+        for (int j = 0; j + 1 < p.k; ++j) R *= p.tb.rg[T[j] * p.tb.n + T[j + 1]];
+    } else {
+        record(p.status, p.detail, s);
+    }
+    nlan[s] = R;
+}
+
+// Stream of a lane: the last s with lstart[s] <= lane (binary search; empty streams share their
+// successor's start, so the last one is the stream that owns the lane).
+static __device__ __forceinline__ int64_t stream_of(const int64_t* lstart, int64_t S, int64_t lane) {
+    int64_t lo = 0, hi = S - 1;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) >> 1;
+        if (lstart[mid] <= lane) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Load lane `lane` into the caller's shared arrays (one thread group of `nt` threads, thread index `t`):
+// returns false (uniformly) when the lane is invalid or its term has zero norm.  sS0 / sF: the vectors.
+template <int KE, int NL>
+__device__ bool load_fused(const StepParams& p, int64_t lane, int t, int nt, double2 (*sM)[NL][CHI][CHI],
+                           double2 (*sU)[KE][NL], int (*sMode)[NL], int* sRow, double2* sS0, double2* sF, int* flag,
+                           bool warp) {
+    const int k = p.k, kk = k - 1;
+    const int64_t s = stream_of(p.lstart, p.S, lane);
+    const int32_t* T = p.T + s * k;
+    if (t == 0) {
+        int ok = 1;
+        int64_t e = lane - p.lstart[s];
+        if (e < 0 || e >= p.nlan[s]) ok = 0;
+        int g[KE];
+        for (int j = k - 2; j >= 0 && ok; --j) {
+            const int rk = p.tb.rg[T[j] * p.tb.n + T[j + 1]];
+            g[j] = (int)(e % rk);
+            e /= rk;
+        }
+        const int fid = p.fid[s];
+        const int rfv = ok ? p.tb.rf[fid * p.tb.n + T[k - 1]] : 1;
+        const int i_f = (int)(e % rfv), i_0 = (int)(e / rfv);
+        if (ok) {
+            for (int c = 0; c < k; ++c)
+                for (int l = 0; l < NL; ++l) {
+                    const double2* src = c + 1 < k
+                        ? p.tb.gops + ((((int64_t)T[c] * p.tb.n + T[c + 1]) * 4 + g[c]) * p.L + l) * CHI * CHI
+                        : p.tb.ops + ((int64_t)T[c] * p.L + l) * CHI * CHI;
+                    for (int ab = 0; ab < CHI * CHI; ++ab) sM[c][l][ab / CHI][ab % CHI] = src[ab];
+                }
+            const double2* v0 = p.tb.pre + ((int64_t)T[0] * 2 + i_0) * CHI;
+            const double2* f0 = p.tb.suf + (((int64_t)fid * p.tb.n + T[k - 1]) * 2 + i_f) * CHI;
+            sS0[0] = v0[0]; sS0[1] = v0[1]; sF[0] = f0[0]; sF[1] = f0[1];
+            // norm of the term: <f (x) f*| E_{k-1} ... E_0 |s0 (x) s0*>, E_j = sum_l M (x) M*
+            double2 v[4];
+            for (int a = 0; a < 2; ++a)
+                for (int b = 0; b < 2; ++b)
+                    v[a * 2 + b] = cmul(sS0[a], make_double2(sS0[b].x, -sS0[b].y));
+            for (int c = 0; c < k; ++c) {
+                double2 nv[4];
+                for (int a = 0; a < 4; ++a) nv[a] = make_double2(0.0, 0.0);
+                for (int l = 0; l < NL; ++l)
+                    for (int t1 = 0; t1 < 2; ++t1)
+                        for (int u1 = 0; u1 < 2; ++u1)
+                            for (int s1 = 0; s1 < 2; ++s1)
+                                for (int v1 = 0; v1 < 2; ++v1) {
+                                    const double2 mc = sM[c][l][u1][v1];
+                                    nv[t1 * 2 + u1] = cmac(nv[t1 * 2 + u1], cmul(sM[c][l][t1][s1],
+                                                                                 make_double2(mc.x, -mc.y)),
+                                                           v[s1 * 2 + v1]);
+                                }
+                for (int a = 0; a < 4; ++a) v[a] = nv[a];
+            }
+            double norm2 = 0.0;
+            for (int a = 0; a < 2; ++a)
+                for (int b = 0; b < 2; ++b) {
+                    const double2 fa = sF[a], fb = sF[b];
+                    const double2 w = cmul(make_double2(fa.x, -fa.y), fb);       // conj(f_a f_b*) = f_a* f_b
+                    norm2 += w.x * v[a * 2 + b].x - w.y * v[a * 2 + b].y;
+                }
+            const double sc = (sF[0].x * sF[0].x + sF[0].y * sF[0].y + sF[1].x * sF[1].x + sF[1].y * sF[1].y) *
+                              (sS0[0].x * sS0[0].x + sS0[0].y * sS0[0].y + sS0[1].x * sS0[1].x + sS0[1].y * sS0[1].y);
+            if (!(norm2 > 1e-14 * (sc > 1.0 ? sc : 1.0))) ok = 0;
+        }
+        *flag = ok;
+    }
+    if (warp) __syncwarp(); else __syncthreads();
+    if (!*flag) return false;
+    int bad = 0;
+    if (t < k * NL) {
+        const int j = t / NL, l = t % NL;
+        const int md = p.modes[T[j] * p.L + l];
+        if (md < 0 || md >= p.M) bad = 1;
+        else sMode[j][l] = md;
+    }
+    if (t < kk) {
+        const int64_t r = p.rows[s * p.rows_stride + t];
+        if (r < 0 || r >= p.m) bad = 1;
+        else sRow[t] = (int)r;
+    }
+    if (bad) { atomicOr(flag, 2); record(p.status, p.detail, lane); }
+    if (warp) __syncwarp(); else __syncthreads();
+    if (*flag & 2) return false;
+    for (int idx = t; idx < kk * k * NL; idx += nt) {
+        const int i = idx / (k * NL), rem = idx % (k * NL);
+        const int j = rem / NL, l = rem % NL;
+        sU[i][j][l] = p.UT[(int64_t)sMode[j][l] * p.m + sRow[i]];
+    }
+    if (warp) __syncwarp(); else __syncthreads();
+    return true;
+}
+
+template <int NL>
+__global__ void __launch_bounds__(32 * WW) emitter_step_warp_kernel(StepParams p) {
+    constexpr int KE = 8;
+    __shared__ double2 wM[WW][KE][NL][CHI][CHI];
+    __shared__ double2 wU[WW][KE][KE][NL];
+    __shared__ double2 wT[WW][KE][NL];
+    __shared__ double2 wS0[WW][2], wF[WW][2];
+    __shared__ int wMode[WW][KE][NL];
+    __shared__ int wRow[WW][KE];
+    __shared__ int wFlag[WW];
+    const int lid = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int k = p.k, kk = k - 1;
+    for (int64_t lane = (int64_t)blockIdx.x * WW + wid; lane < p.nl; lane += (int64_t)gridDim.x * WW) {
+        if (!load_fused<KE, NL>(p, lane, lid, 32, wM[wid], wU[wid], wMode[wid], wRow[wid], wS0[wid], wF[wid],
+                                &wFlag[wid], true)) {
+            for (int rho = lid; rho < p.m; rho += 32) p.amp[lane * p.m + rho] = make_double2(0.0, 0.0);
+            __syncwarp();
+            continue;
+        }
+        const int64_t D = kk >= 1 ? ((int64_t)1 << (kk - 1)) : 1;
+        int64_t t0, t1;
+        if (D >= 32) { const int64_t per = D / 32; t0 = lid * per; t1 = t0 + per; }
+        else { t0 = lid; t1 = lid < D ? lid + 1 : lid; }
+        double2 acc[KE][NL];
+        walk<KE, NL>(wM[wid], wU[wid], k, t0, t1, wS0[wid][0], wS0[wid][1], make_double2(wF[wid][0].x, -wF[wid][0].y),
+                     make_double2(wF[wid][1].x, -wF[wid][1].y), acc);
+        const double norm = kk >= 1 ? ldexp(1.0, -(kk - 1)) : 1.0;
+#pragma unroll
+        for (int j = 0; j < KE; ++j)
+#pragma unroll
+            for (int l = 0; l < NL; ++l) {
+                double2 x = acc[j][l];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    x.x += __shfl_xor_sync(0xffffffffu, x.x, o);
+                    x.y += __shfl_xor_sync(0xffffffffu, x.y, o);
+                }
+                if (lid == 0 && j < k) wT[wid][j][l] = make_double2(x.x * norm, x.y * norm);
+            }
+        __syncwarp();
+        for (int rho = lid; rho < p.m; rho += 32) {
+            double2 a = make_double2(0.0, 0.0);
+            for (int c = 0; c < k; ++c)
+#pragma unroll
+                for (int l = 0; l < NL; ++l) a = cmac(a, p.UT[(int64_t)wMode[wid][c][l] * p.m + rho], wT[wid][c][l]);
+            p.amp[lane * p.m + rho] = a;
+        }
+        __syncwarp();
+    }
+}
+
+template <int KE, int NL>
+__global__ void __launch_bounds__(THREADS) emitter_step_kernel(StepParams p) {
+    __shared__ double2 sM[KE][NL][CHI][CHI];
+    __shared__ double2 sU[KE][KE][NL];
+    __shared__ double2 red[NWARP][KE][NL];
+    __shared__ double2 sT[KE][NL];
+    __shared__ double2 sS0[2], sF[2];
+    __shared__ int sMode[KE][NL];
+    __shared__ int sRow[KE];
+    __shared__ int flag;
+    const int tid = threadIdx.x, lid = tid & 31, wid = tid >> 5;
+    const int k = p.k, kk = k - 1;
+    for (int64_t lane = blockIdx.x; lane < p.nl; lane += gridDim.x) {
+        if (!load_fused<KE, NL>(p, lane, tid, THREADS, sM, sU, sMode, sRow, sS0, sF, &flag, false)) {
+            for (int rho = tid; rho < p.m; rho += THREADS) p.amp[lane * p.m + rho] = make_double2(0.0, 0.0);
+            __syncthreads();
+            continue;
+        }
+        const int64_t D = kk >= 1 ? ((int64_t)1 << (kk - 1)) : 1;
+        int64_t t0, t1;
+        if (D >= THREADS) { const int64_t per = D / THREADS; t0 = tid * per; t1 = t0 + per; }
+        else { t0 = tid; t1 = tid < D ? tid + 1 : tid; }
+        double2 acc[KE][NL];
+        walk<KE, NL>(sM, sU, k, t0, t1, sS0[0], sS0[1], make_double2(sF[0].x, -sF[0].y), make_double2(sF[1].x, -sF[1].y),
+                     acc);
+#pragma unroll
+        for (int j = 0; j < KE; ++j)
+#pragma unroll
+            for (int l = 0; l < NL; ++l) {
+                double2 x = acc[j][l];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    x.x += __shfl_xor_sync(0xffffffffu, x.x, o);
+                    x.y += __shfl_xor_sync(0xffffffffu, x.y, o);
+                }
+                if (lid == 0 && j < k) red[wid][j][l] = x;
+            }
+        __syncthreads();
+        const double norm = kk >= 1 ? ldexp(1.0, -(kk - 1)) : 1.0;
+        if (tid < k * NL) {
+            const int j = tid / NL, l = tid % NL;
+            double2 x = make_double2(0.0, 0.0);
+            for (int w = 0; w < NWARP; ++w) { x.x += red[w][j][l].x; x.y += red[w][j][l].y; }
+            sT[j][l] = make_double2(x.x * norm, x.y * norm);
+        }
+        __syncthreads();
+        for (int rho = tid; rho < p.m; rho += THREADS) {
+            double2 a = make_double2(0.0, 0.0);
+            for (int c = 0; c < k; ++c)
+#pragma unroll
+                for (int l = 0; l < NL; ++l) a = cmac(a, p.UT[(int64_t)sMode[c][l] * p.m + rho], sT[c][l]);
+            p.amp[lane * p.m + rho] = a;
+        }
+        __syncthreads();
+    }
+}
+
+template <class K>
+static int occupancy_grid(K kernel, int threads, int64_t units, int64_t* grid) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0) != cudaSuccess) return PE_ERR_CUDA;
+    if (per < 1) return PE_ERR_SIZE;
+    *grid = (int64_t)sms * per;
+    if (*grid > units) *grid = units;
+    if (*grid < 1) *grid = 1;
+    return PE_OK;
+}
+
 template <int NL>
 static int launch_amp_warp(const Params& p, cudaStream_t st) {
     int dev = 0, sms = 0, per = 0;
@@ -402,5 +684,83 @@ extern "C" int pe_emitter_weights(const double* d_ut, int m, int M, const int64_
     const int T = 256;
     emitter_weights_kernel<<<(unsigned)((total + T - 1) / T), T, 0, st>>>((const double2*)d_amp, d_lstart, d_nlan, S, m,
                                                                           nl, d_w, p.status, p.detail);
+    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+}
+
+extern "C" int pe_emitter_count(const int32_t* d_T, const int32_t* d_fid, int64_t S, int k, const int32_t* d_rg,
+                                const int32_t* d_r0, const int32_t* d_rf, int n, int nf, int64_t* d_nlan,
+                                void* d_workspace, size_t workspace_bytes, void* stream) {
+    if (S < 0 || k < 1 || k > MAXK || n < 1 || k > n || nf < 1) return PE_ERR_SIZE;
+    if (!d_T || !d_fid || !d_rg || !d_r0 || !d_rf || !d_nlan || !d_workspace) return PE_ERR_ARG;
+    if (workspace_bytes < 256) return PE_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(d_workspace, 0, 256, st) != cudaSuccess) return PE_ERR_CUDA;
+    if (S == 0) return PE_OK;
+    StepParams p = {};
+    p.T = d_T; p.fid = d_fid; p.S = S; p.k = k;
+    p.tb.rg = d_rg; p.tb.r0 = d_r0; p.tb.rf = d_rf; p.tb.n = n; p.tb.nf = nf;
+    p.status = (int*)((char*)d_workspace + 8);
+    p.detail = (long long*)((char*)d_workspace + 16);
+    emitter_count_kernel<<<(unsigned)((S + 255) / 256), 256, 0, st>>>(p, d_nlan);
+    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+}
+
+extern "C" int pe_emitter_step(const double* d_ut, int m, int M, const int64_t* d_rows, int rows_stride,
+                               const int32_t* d_T, const int32_t* d_fid, const int32_t* d_modes, int64_t S, int k,
+                               int L, int chi, const double* d_gops, const int32_t* d_rg, const double* d_ops,
+                               const double* d_pre, const int32_t* d_r0, const double* d_suf, const int32_t* d_rf,
+                               int n, int nf, const int64_t* d_lstart, const int64_t* d_nlan, int64_t nl,
+                               double* d_amp, double* d_w, void* d_workspace, size_t workspace_bytes, void* stream) {
+    if (chi != CHI) return PE_ERR_SIZE;
+    if (L < 1 || L > 2 || k < 1 || k > MAXK || n < 1 || k > n || nf < 1) return PE_ERR_SIZE;
+    if (m < 1 || M < 1 || S < 0 || nl < 0 || rows_stride < (k > 1 ? k - 1 : 0)) return PE_ERR_ARG;
+    if (!d_ut || !d_T || !d_fid || !d_modes || !d_gops || !d_rg || !d_ops || !d_pre || !d_r0 || !d_suf || !d_rf ||
+        !d_lstart || !d_nlan || !d_amp || !d_w || !d_workspace || (k > 1 && !d_rows))
+        return PE_ERR_ARG;
+    if (workspace_bytes < 256) return PE_ERR_SIZE;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (S == 0) return PE_OK;
+    StepParams p;
+    p.UT = (const double2*)d_ut; p.m = m; p.M = M; p.rows = d_rows; p.rows_stride = rows_stride;
+    p.T = d_T; p.fid = d_fid; p.modes = d_modes; p.S = S; p.k = k; p.L = L;
+    p.tb.gops = (const double2*)d_gops; p.tb.rg = d_rg; p.tb.ops = (const double2*)d_ops;
+    p.tb.pre = (const double2*)d_pre; p.tb.r0 = d_r0; p.tb.suf = (const double2*)d_suf; p.tb.rf = d_rf;
+    p.tb.n = n; p.tb.nf = nf;
+    p.lstart = d_lstart; p.nlan = d_nlan; p.nl = nl; p.amp = (double2*)d_amp;
+    p.status = (int*)((char*)d_workspace + 8);
+    p.detail = (long long*)((char*)d_workspace + 16);
+    int64_t grid = 0;
+    int rc = PE_OK;
+    if (nl > 0) {
+        if (k <= 8) {
+            if (L == 1) {
+                if ((rc = occupancy_grid(emitter_step_warp_kernel<1>, 32 * WW, (nl + WW - 1) / WW, &grid)) != PE_OK) return rc;
+                emitter_step_warp_kernel<1><<<(unsigned)grid, 32 * WW, 0, st>>>(p);
+            } else {
+                if ((rc = occupancy_grid(emitter_step_warp_kernel<2>, 32 * WW, (nl + WW - 1) / WW, &grid)) != PE_OK) return rc;
+                emitter_step_warp_kernel<2><<<(unsigned)grid, 32 * WW, 0, st>>>(p);
+            }
+        } else if (k <= 16) {
+            if (L == 1) {
+                if ((rc = occupancy_grid(emitter_step_kernel<16, 1>, THREADS, nl, &grid)) != PE_OK) return rc;
+                emitter_step_kernel<16, 1><<<(unsigned)grid, THREADS, 0, st>>>(p);
+            } else {
+                if ((rc = occupancy_grid(emitter_step_kernel<16, 2>, THREADS, nl, &grid)) != PE_OK) return rc;
+                emitter_step_kernel<16, 2><<<(unsigned)grid, THREADS, 0, st>>>(p);
+            }
+        } else {
+            if (L == 1) {
+                if ((rc = occupancy_grid(emitter_step_kernel<24, 1>, THREADS, nl, &grid)) != PE_OK) return rc;
+                emitter_step_kernel<24, 1><<<(unsigned)grid, THREADS, 0, st>>>(p);
+            } else {
+                if ((rc = occupancy_grid(emitter_step_kernel<24, 2>, THREADS, nl, &grid)) != PE_OK) return rc;
+                emitter_step_kernel<24, 2><<<(unsigned)grid, THREADS, 0, st>>>(p);
+            }
+        }
+        if (cudaGetLastError() != cudaSuccess) return PE_ERR_CUDA;
+    }
+    const int64_t total = S * (int64_t)m;
+    emitter_weights_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>((const double2*)d_amp, d_lstart, d_nlan, S,
+                                                                            m, nl, d_w, p.status, p.detail);
     return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
 }

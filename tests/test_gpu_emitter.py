@@ -113,3 +113,30 @@ def test_an_out_of_range_mode_is_reported_not_faulted():
                                 s0.data_ptr(), s0.data_ptr(), mats.data_ptr(), 1, lane.data_ptr(), lane.data_ptr(),
                                 lane.data_ptr(), nlan.data_ptr(), 1, amp.data_ptr(), w.data_ptr(), ws.data_ptr(), 256,
                                 N.stream_handle(torch.device(DEV))) == N.PE_ERR_SIZE            # chi = 3
+
+
+@pytest.mark.parametrize(("n", "L", "ks", "final"), [(10, 2, (1, 2, 6, 8), True), (12, 1, (9, 12), False),
+                                                    (14, 2, (12,), True), (20, 1, (17, 18), False)])
+def test_fused_steps_match_the_oracle(n, L, ks, final):
+    """pe_emitter_count + pe_emitter_step (terms assembled on the device from the per-state tables)."""
+    from photonic_engines_b200.clifford.emitter import fused_step_weights, tables_for
+    st, rng = _random_emitter(n, L, 300 + n + L, final)
+    U = O.haar_unitary(st.m, 9 + n)
+    Ud = torch.as_tensor(U, device=DEV)
+    ut = torch.view_as_real(Ud.transpose(0, 1).contiguous()).contiguous()
+    tb = tables_for(st, DEV)
+    S = 4
+    for k in ks:
+        T = torch.tensor([sorted(rng.choice(n, size=k, replace=False).tolist()) for _ in range(S)], dtype=torch.int32)
+        rows = torch.as_tensor(rng.integers(0, st.m, size=(S, n)), dtype=torch.int64)
+        fid = torch.as_tensor(rng.integers(0, 1 if final else 2, size=S), dtype=torch.int32)
+        ws = torch.zeros(256, dtype=torch.uint8, device=DEV)
+        got, _ = fused_step_weights(ut, st.m, st, T.to(DEV), rows.to(DEV), fid.to(DEV), tb, ws)
+        assert N.read_status(ws)[0] == 0
+        got = got.cpu().numpy()
+        for s in range(S):
+            fv = None if final else torch.eye(2, dtype=torch.complex128)[int(fid[s])]
+            kept, s0, mats, f = gap_terms(st, T[s].tolist(), fv)
+            colmode = np.array([list(st.modes[j]) for j in kept])
+            want = EO.matrix_weights(U, colmode, rows[s, :k - 1].tolist(), s0.numpy(), mats.numpy(), f.numpy())
+            assert _rel(got[s], want) < 1e-10, (n, L, k, s)
