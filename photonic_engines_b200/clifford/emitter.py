@@ -20,6 +20,7 @@ from __future__ import annotations
 
 import math
 
+import numpy as np
 import torch
 
 from .. import _native as N
@@ -180,6 +181,14 @@ class _Tables:
         self.rg32, self.r032, self.rf32 = (x.to(device, torch.int32).contiguous() for x in (RG, R0, RF))
         self.modes32 = torch.tensor([list(mk) for mk in state.modes], dtype=torch.int32, device=device)
         self.n, self.nf = n, len(finals)
+        self.rg_np, self.r0_np, self.rf_np = RG.numpy(), R0.numpy(), RF.numpy()       # host copies of the ranks
+
+    def counts(self, T, fid):
+        """Terms per stream (int64 numpy [S]) for placed slots T [S, k] and final ids fid [S] (numpy)."""
+        R = self.r0_np[T[:, 0]] * self.rf_np[fid, T[:, -1]]
+        if T.shape[1] > 1:
+            R = R * np.prod(self.rg_np[T[:, :-1], T[:, 1:]], axis=1)
+        return R.astype(np.int64)
 
     def lanes(self, T: torch.Tensor, fid: torch.Tensor):
         """Every stream's pure terms for its placed slots T [S, k] (sorted, device) and final ids fid [S]:
@@ -302,23 +311,33 @@ def fused_step_weights(ut: torch.Tensor, m: int, state: EmitterMPS, T: torch.Ten
             "pe_emitter_count")
     lstart = torch.cumsum(nlan, 0) - nlan
     nl = int(nlan.sum())
+    w = _step_launch(ut, m, state, T, rows, fid32, tables, lstart, nlan, nl, ws, events)
+    return w, nl
+
+
+def _step_launch(ut: torch.Tensor, m: int, state: EmitterMPS, T: torch.Tensor, rows: torch.Tensor, fid32: torch.Tensor,
+                 tables: _Tables, lstart: torch.Tensor, nlan: torch.Tensor, nl: int, ws: torch.Tensor,
+                 events: list | None = None) -> torch.Tensor:
+    """pe_emitter_step for given lane offsets; returns w [S, m]."""
+    dev = T.device
+    S, k = T.shape
     amp = torch.empty(max(nl, 1), m, dtype=C128, device=dev)
     w = torch.empty(S, m, dtype=torch.float64, device=dev)
     if events is not None:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-    rc = L_.pe_emitter_step(N.ptr(ut), m, int(ut.shape[0]), N.ptr(rows), int(rows.shape[1]), N.ptr(T), N.ptr(fid32),
-                            N.ptr(tables.modes32), S, k, state.num_labels, state.chi,
-                            N.ptr(torch.view_as_real(tables.GOPS)), N.ptr(tables.rg32),
-                            N.ptr(torch.view_as_real(tables.ops)), N.ptr(torch.view_as_real(tables.PRE)),
-                            N.ptr(tables.r032), N.ptr(torch.view_as_real(tables.SUF)), N.ptr(tables.rf32), tables.n,
-                            tables.nf, N.ptr(lstart), N.ptr(nlan), nl, N.ptr(torch.view_as_real(amp)), N.ptr(w),
-                            N.ptr(ws), int(ws.numel()), st)
+    rc = N.load().pe_emitter_step(N.ptr(ut), m, int(ut.shape[0]), N.ptr(rows), int(rows.shape[1]), N.ptr(T),
+                                  N.ptr(fid32), N.ptr(tables.modes32), S, k, state.num_labels, state.chi,
+                                  N.ptr(torch.view_as_real(tables.GOPS)), N.ptr(tables.rg32),
+                                  N.ptr(torch.view_as_real(tables.ops)), N.ptr(torch.view_as_real(tables.PRE)),
+                                  N.ptr(tables.r032), N.ptr(torch.view_as_real(tables.SUF)), N.ptr(tables.rf32),
+                                  tables.n, tables.nf, N.ptr(lstart), N.ptr(nlan), nl, N.ptr(torch.view_as_real(amp)),
+                                  N.ptr(w), N.ptr(ws), int(ws.numel()), N.stream_handle(dev))
     N.check(rc, "pe_emitter_step")
     if events is not None:
         e1.record()
         events.append((e0, e1, nl, k))
-    return w, nl
+    return w
 
 
 def step_weights(U_t: torch.Tensor, state: EmitterMPS, Tsorted: torch.Tensor, rows: torch.Tensor, fid: torch.Tensor,
@@ -415,15 +434,21 @@ def emitter_sample(state: EmitterMPS, U: torch.Tensor, shots: int, generator: to
     rows = torch.zeros((S, n), dtype=torch.long)
     rows_d = torch.zeros((S, max(n, 1)), dtype=torch.int64, device=dev)
     tables = tables_for(state, dev)
-    sigma_d, fid32 = sigma.to(dev), fid.to(dev, torch.int32)
+    sigma_np, fid_np = sigma.numpy(), fid.numpy()
+    fid32 = fid.to(dev, torch.int32)
     ut = torch.view_as_real(U_t.transpose(0, 1).contiguous()).contiguous()
     wsb = int(N.load().pe_emitter_workspace_bytes())
-    wss = torch.empty(n, wsb, dtype=torch.uint8, device=dev)           # one status word per step, read once
+    wss = torch.zeros(n, wsb, dtype=torch.uint8, device=dev)           # one status word per step, read once
     stats = {"R": []}                                                    # mean lanes (pure terms) per stream
     events = [] if return_stats else None
     for k in range(1, n + 1):
-        Tsorted = torch.sort(sigma_d[:, :k], dim=1).values.to(torch.int32)
-        w, nl = fused_step_weights(ut, m, state, Tsorted, rows_d, fid32, tables, wss[k - 1], events)
+        T_np = np.sort(sigma_np[:, :k], axis=1)
+        nlan_np = tables.counts(T_np, fid_np)                            # terms per stream, on the host
+        nl = int(nlan_np.sum())
+        T_d = torch.from_numpy(T_np.astype(np.int32)).to(dev)
+        nlan = torch.from_numpy(nlan_np).to(dev)
+        lstart = torch.from_numpy(np.cumsum(nlan_np) - nlan_np).to(dev)
+        w = _step_launch(ut, m, state, T_d, rows_d, fid32, tables, lstart, nlan, nl, wss[k - 1], events)
         w = w.cpu()
         w = w.clamp_min(0)
         w = w / w.sum(dim=1, keepdim=True)

@@ -380,80 +380,89 @@ static __device__ __forceinline__ int64_t stream_of(const int64_t* lstart, int64
     return lo;
 }
 
-// Load lane `lane` into the caller's shared arrays (one thread group of `nt` threads, thread index `t`):
-// returns false (uniformly) when the lane is invalid or its term has zero norm.  sS0 / sF: the vectors.
+// Load lane `lane` into the caller's shared arrays (one thread group of `nt` threads, thread index `t`,
+// whose first warp holds threads 0..31): returns false (uniformly) when the lane is invalid or its term has
+// zero norm.  Thread 0 decodes the term index into sG (gap choices) and sI (i0, if); the group gathers the
+// matrices and vectors; lanes 0..3 of the first warp run the norm's transfer chain (one component each).
 template <int KE, int NL>
 __device__ bool load_fused(const StepParams& p, int64_t lane, int t, int nt, double2 (*sM)[NL][CHI][CHI],
                            double2 (*sU)[KE][NL], int (*sMode)[NL], int* sRow, double2* sS0, double2* sF, int* flag,
-                           bool warp) {
+                           int* sG, bool warp) {
     const int k = p.k, kk = k - 1;
     const int64_t s = stream_of(p.lstart, p.S, lane);
     const int32_t* T = p.T + s * k;
+    const int fid = p.fid[s];
     if (t == 0) {
         int ok = 1;
         int64_t e = lane - p.lstart[s];
         if (e < 0 || e >= p.nlan[s]) ok = 0;
-        int g[KE];
         for (int j = k - 2; j >= 0 && ok; --j) {
             const int rk = p.tb.rg[T[j] * p.tb.n + T[j + 1]];
-            g[j] = (int)(e % rk);
+            sG[j] = (int)(e % rk);
             e /= rk;
         }
-        const int fid = p.fid[s];
-        const int rfv = ok ? p.tb.rf[fid * p.tb.n + T[k - 1]] : 1;
-        const int i_f = (int)(e % rfv), i_0 = (int)(e / rfv);
         if (ok) {
-            for (int c = 0; c < k; ++c)
-                for (int l = 0; l < NL; ++l) {
-                    const double2* src = c + 1 < k
-                        ? p.tb.gops + ((((int64_t)T[c] * p.tb.n + T[c + 1]) * 4 + g[c]) * p.L + l) * CHI * CHI
-                        : p.tb.ops + ((int64_t)T[c] * p.L + l) * CHI * CHI;
-                    for (int ab = 0; ab < CHI * CHI; ++ab) sM[c][l][ab / CHI][ab % CHI] = src[ab];
-                }
-            const double2* v0 = p.tb.pre + ((int64_t)T[0] * 2 + i_0) * CHI;
-            const double2* f0 = p.tb.suf + (((int64_t)fid * p.tb.n + T[k - 1]) * 2 + i_f) * CHI;
-            sS0[0] = v0[0]; sS0[1] = v0[1]; sF[0] = f0[0]; sF[1] = f0[1];
-            // norm of the term: <f (x) f*| E_{k-1} ... E_0 |s0 (x) s0*>, E_j = sum_l M (x) M*
-            double2 v[4];
-            for (int a = 0; a < 2; ++a)
-                for (int b = 0; b < 2; ++b)
-                    v[a * 2 + b] = cmul(sS0[a], make_double2(sS0[b].x, -sS0[b].y));
-            for (int c = 0; c < k; ++c) {
-                double2 nv[4];
-                for (int a = 0; a < 4; ++a) nv[a] = make_double2(0.0, 0.0);
-                for (int l = 0; l < NL; ++l)
-                    for (int t1 = 0; t1 < 2; ++t1)
-                        for (int u1 = 0; u1 < 2; ++u1)
-                            for (int s1 = 0; s1 < 2; ++s1)
-                                for (int v1 = 0; v1 < 2; ++v1) {
-                                    const double2 mc = sM[c][l][u1][v1];
-                                    nv[t1 * 2 + u1] = cmac(nv[t1 * 2 + u1], cmul(sM[c][l][t1][s1],
-                                                                                 make_double2(mc.x, -mc.y)),
-                                                           v[s1 * 2 + v1]);
-                                }
-                for (int a = 0; a < 4; ++a) v[a] = nv[a];
-            }
-            double norm2 = 0.0;
-            for (int a = 0; a < 2; ++a)
-                for (int b = 0; b < 2; ++b) {
-                    const double2 fa = sF[a], fb = sF[b];
-                    const double2 w = cmul(make_double2(fa.x, -fa.y), fb);       // conj(f_a f_b*) = f_a* f_b
-                    norm2 += w.x * v[a * 2 + b].x - w.y * v[a * 2 + b].y;
-                }
-            const double sc = (sF[0].x * sF[0].x + sF[0].y * sF[0].y + sF[1].x * sF[1].x + sF[1].y * sF[1].y) *
-                              (sS0[0].x * sS0[0].x + sS0[0].y * sS0[0].y + sS0[1].x * sS0[1].x + sS0[1].y * sS0[1].y);
-            if (!(norm2 > 1e-14 * (sc > 1.0 ? sc : 1.0))) ok = 0;
+            const int rfv = p.tb.rf[fid * p.tb.n + T[k - 1]];
+            sG[KE] = (int)(e / rfv);            // i0
+            sG[KE + 1] = (int)(e % rfv);        // if
         }
         *flag = ok;
     }
     if (warp) __syncwarp(); else __syncthreads();
     if (!*flag) return false;
+    for (int idx = t; idx < k * NL * CHI * CHI; idx += nt) {
+        const int c = idx / (NL * CHI * CHI), rem = idx % (NL * CHI * CHI);
+        const int l = rem / (CHI * CHI), ab = rem % (CHI * CHI);
+        const double2* src = c + 1 < k
+            ? p.tb.gops + ((((int64_t)T[c] * p.tb.n + T[c + 1]) * 4 + sG[c]) * p.L + l) * CHI * CHI
+            : p.tb.ops + ((int64_t)T[c] * p.L + l) * CHI * CHI;
+        sM[c][l][ab / CHI][ab % CHI] = src[ab];
+    }
+    if (t < 2) sS0[t] = p.tb.pre[((int64_t)T[0] * 2 + sG[KE]) * CHI + t];
+    else if (t < 4) sF[t - 2] = p.tb.suf[(((int64_t)fid * p.tb.n + T[k - 1]) * 2 + sG[KE + 1]) * CHI + (t - 2)];
+    if (warp) __syncwarp(); else __syncthreads();
+    if (t < 32) {
+        // norm^2 = <f (x) f*| E_{k-1} ... E_0 |s0 (x) s0*>, E_c = sum_l M_{c,l} (x) M_{c,l}*; lane j < 4 holds
+        // component j = (t1, u1) of the transfer vector (lanes 4..31 compute a copy of component j % 4)
+        const int j = t & 3, t1 = j >> 1, u1 = j & 1;
+        double2 v = cmul(sS0[t1], make_double2(sS0[u1].x, -sS0[u1].y));
+        for (int c = 0; c < k; ++c) {
+            double2 vs[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                vs[q].x = __shfl_sync(0xffffffffu, v.x, (t & ~3) + q);
+                vs[q].y = __shfl_sync(0xffffffffu, v.y, (t & ~3) + q);
+            }
+            double2 nv = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int l = 0; l < NL; ++l)
+#pragma unroll
+                for (int s1 = 0; s1 < 2; ++s1)
+#pragma unroll
+                    for (int v1 = 0; v1 < 2; ++v1) {
+                        const double2 mc = sM[c][l][u1][v1];
+                        nv = cmac(nv, cmul(sM[c][l][t1][s1], make_double2(mc.x, -mc.y)), vs[s1 * 2 + v1]);
+                    }
+            v = nv;
+        }
+        const double2 w = cmul(make_double2(sF[t1].x, -sF[t1].y), sF[u1]);      // f_a* f_b
+        double part = w.x * v.x - w.y * v.y;
+        part += __shfl_xor_sync(0xffffffffu, part, 1);
+        part += __shfl_xor_sync(0xffffffffu, part, 2);
+        if (t == 0) {
+            const double sc = (sF[0].x * sF[0].x + sF[0].y * sF[0].y + sF[1].x * sF[1].x + sF[1].y * sF[1].y) *
+                              (sS0[0].x * sS0[0].x + sS0[0].y * sS0[0].y + sS0[1].x * sS0[1].x + sS0[1].y * sS0[1].y);
+            if (!(part > 1e-14 * (sc > 1.0 ? sc : 1.0))) *flag = 0;
+        }
+    }
+    if (warp) __syncwarp(); else __syncthreads();
+    if (!*flag) return false;
     int bad = 0;
     if (t < k * NL) {
-        const int j = t / NL, l = t % NL;
-        const int md = p.modes[T[j] * p.L + l];
+        const int jj = t / NL, l = t % NL;
+        const int md = p.modes[T[jj] * p.L + l];
         if (md < 0 || md >= p.M) bad = 1;
-        else sMode[j][l] = md;
+        else sMode[jj][l] = md;
     }
     if (t < kk) {
         const int64_t r = p.rows[s * p.rows_stride + t];
@@ -465,8 +474,8 @@ __device__ bool load_fused(const StepParams& p, int64_t lane, int t, int nt, dou
     if (*flag & 2) return false;
     for (int idx = t; idx < kk * k * NL; idx += nt) {
         const int i = idx / (k * NL), rem = idx % (k * NL);
-        const int j = rem / NL, l = rem % NL;
-        sU[i][j][l] = p.UT[(int64_t)sMode[j][l] * p.m + sRow[i]];
+        const int jj = rem / NL, l = rem % NL;
+        sU[i][jj][l] = p.UT[(int64_t)sMode[jj][l] * p.m + sRow[i]];
     }
     if (warp) __syncwarp(); else __syncthreads();
     return true;
@@ -482,11 +491,12 @@ __global__ void __launch_bounds__(32 * WW) emitter_step_warp_kernel(StepParams p
     __shared__ int wMode[WW][KE][NL];
     __shared__ int wRow[WW][KE];
     __shared__ int wFlag[WW];
+    __shared__ int wG[WW][KE + 2];
     const int lid = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int k = p.k, kk = k - 1;
     for (int64_t lane = (int64_t)blockIdx.x * WW + wid; lane < p.nl; lane += (int64_t)gridDim.x * WW) {
         if (!load_fused<KE, NL>(p, lane, lid, 32, wM[wid], wU[wid], wMode[wid], wRow[wid], wS0[wid], wF[wid],
-                                &wFlag[wid], true)) {
+                                &wFlag[wid], wG[wid], true)) {
             for (int rho = lid; rho < p.m; rho += 32) p.amp[lane * p.m + rho] = make_double2(0.0, 0.0);
             __syncwarp();
             continue;
@@ -533,10 +543,11 @@ __global__ void __launch_bounds__(THREADS) emitter_step_kernel(StepParams p) {
     __shared__ int sMode[KE][NL];
     __shared__ int sRow[KE];
     __shared__ int flag;
+    __shared__ int sG[KE + 2];
     const int tid = threadIdx.x, lid = tid & 31, wid = tid >> 5;
     const int k = p.k, kk = k - 1;
     for (int64_t lane = blockIdx.x; lane < p.nl; lane += gridDim.x) {
-        if (!load_fused<KE, NL>(p, lane, tid, THREADS, sM, sU, sMode, sRow, sS0, sF, &flag, false)) {
+        if (!load_fused<KE, NL>(p, lane, tid, THREADS, sM, sU, sMode, sRow, sS0, sF, &flag, sG, false)) {
             for (int rho = tid; rho < p.m; rho += THREADS) p.amp[lane * p.m + rho] = make_double2(0.0, 0.0);
             __syncthreads();
             continue;
