@@ -141,6 +141,89 @@ __device__ __forceinline__ void walk(const double2 (*sM)[NL][CHI][CHI], const do
     }
 }
 
+// The same walk with the stored backward chain and the trace accumulators in shared memory (too many
+// values for registers at 16-24 columns): q[(c * 2 + a) * nt + t] and acc[(c * NL + l) * nt + t] for
+// thread t of nt, consecutive threads at consecutive addresses.  The column sums stay in registers.
+template <int KE, int NL>
+__device__ __forceinline__ void walk_shared(const double2 (*sM)[NL][CHI][CHI], const double2 (*sU)[KE][NL], int k,
+                                            int64_t t0, int64_t t1, double2 s00, double2 s01, double2 fc0,
+                                            double2 fc1, double2* q, double2* acc, int t, int nt) {
+    const int kk = k - 1;
+    for (int j = 0; j < k * NL; ++j) acc[j * nt + t] = make_double2(0.0, 0.0);
+    if (t0 >= t1) return;
+    double2 cs[KE][NL];
+    uint64_t g = (uint64_t)(t0 ^ (t0 >> 1));
+#pragma unroll
+    for (int j = 0; j < KE; ++j)
+#pragma unroll
+        for (int l = 0; l < NL; ++l) {
+            double2 x = make_double2(kk == 0 ? 1.0 : 0.0, 0.0);
+            if (j < k) {
+                for (int i = 0; i < kk; ++i) {
+                    const double d = (i == 0 || !((g >> (i - 1)) & 1)) ? 1.0 : -1.0;
+                    x.x = fma(d, sU[i][j][l].x, x.x);
+                    x.y = fma(d, sU[i][j][l].y, x.y);
+                }
+            }
+            cs[j][l] = x;
+        }
+    double sign = (__popcll(g) & 1) ? -1.0 : 1.0;
+    for (int64_t tt = t0; tt < t1; ++tt) {
+        if (tt > t0) {
+            const int b = __ffsll((long long)tt) - 1;
+            g ^= (uint64_t)1 << b;
+            const double d2 = ((g >> b) & 1) ? -2.0 : 2.0;
+            const int i = b + 1;
+#pragma unroll
+            for (int j = 0; j < KE; ++j)
+#pragma unroll
+                for (int l = 0; l < NL; ++l)
+                    if (j < k) {
+                        cs[j][l].x = fma(d2, sU[i][j][l].x, cs[j][l].x);
+                        cs[j][l].y = fma(d2, sU[i][j][l].y, cs[j][l].y);
+                    }
+            sign = -sign;
+        }
+        double2 u0 = fc0, u1 = fc1;
+#pragma unroll
+        for (int c = KE - 1; c >= 0; --c) {
+            if (c < k) {
+                q[(c * 2) * nt + t] = u0;
+                q[(c * 2 + 1) * nt + t] = u1;
+                double2 n0 = make_double2(0.0, 0.0), n1 = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int l = 0; l < NL; ++l) {
+                    const double2 z0 = cmac(cmul(u0, sM[c][l][0][0]), u1, sM[c][l][1][0]);
+                    const double2 z1 = cmac(cmul(u0, sM[c][l][0][1]), u1, sM[c][l][1][1]);
+                    n0 = cmac(n0, cs[c][l], z0);
+                    n1 = cmac(n1, cs[c][l], z1);
+                }
+                u0 = n0; u1 = n1;
+            }
+        }
+        double2 v0 = s00, v1 = s01;
+#pragma unroll
+        for (int c = 0; c < KE; ++c) {
+            if (c < k) {
+                const double2 qa = q[(c * 2) * nt + t], qb = q[(c * 2 + 1) * nt + t];
+                double2 n0 = make_double2(0.0, 0.0), n1 = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int l = 0; l < NL; ++l) {
+                    const double2 y0 = cmac(cmul(sM[c][l][0][0], v0), sM[c][l][0][1], v1);
+                    const double2 y1 = cmac(cmul(sM[c][l][1][0], v0), sM[c][l][1][1], v1);
+                    const double2 dt = cmac(cmul(qa, y0), qb, y1);
+                    double2& a = acc[(c * NL + l) * nt + t];
+                    a.x = fma(sign, dt.x, a.x);
+                    a.y = fma(sign, dt.y, a.y);
+                    n0 = cmac(n0, cs[c][l], y0);
+                    n1 = cmac(n1, cs[c][l], y1);
+                }
+                v0 = n0; v1 = n1;
+            }
+        }
+    }
+}
+
 template <int KE, int NL>
 __global__ void __launch_bounds__(THREADS) emitter_amp_kernel(Params p) {
     __shared__ double2 sM[KE][NL][CHI][CHI];
@@ -533,54 +616,46 @@ __global__ void __launch_bounds__(32 * WW) emitter_step_warp_kernel(StepParams p
     }
 }
 
+constexpr int STHREADS = 64;          // threads per lane of the wide fused step (more sign vectors each)
 template <int KE, int NL>
-__global__ void __launch_bounds__(THREADS) emitter_step_kernel(StepParams p) {
+__host__ __device__ constexpr size_t step_dyn_smem() { return (size_t)STHREADS * (2 * KE + KE * NL) * sizeof(double2); }
+
+template <int KE, int NL>
+__global__ void __launch_bounds__(STHREADS) emitter_step_kernel(StepParams p) {
+    extern __shared__ __align__(16) unsigned char dyn[];
+    double2* q = reinterpret_cast<double2*>(dyn);                  // [2 KE][STHREADS]
+    double2* acc = q + 2 * KE * STHREADS;                           // [KE NL][STHREADS]
     __shared__ double2 sM[KE][NL][CHI][CHI];
     __shared__ double2 sU[KE][KE][NL];
-    __shared__ double2 red[NWARP][KE][NL];
     __shared__ double2 sT[KE][NL];
     __shared__ double2 sS0[2], sF[2];
     __shared__ int sMode[KE][NL];
     __shared__ int sRow[KE];
     __shared__ int flag;
     __shared__ int sG[KE + 2];
-    const int tid = threadIdx.x, lid = tid & 31, wid = tid >> 5;
+    const int tid = threadIdx.x;
     const int k = p.k, kk = k - 1;
     for (int64_t lane = blockIdx.x; lane < p.nl; lane += gridDim.x) {
-        if (!load_fused<KE, NL>(p, lane, tid, THREADS, sM, sU, sMode, sRow, sS0, sF, &flag, sG, false)) {
-            for (int rho = tid; rho < p.m; rho += THREADS) p.amp[lane * p.m + rho] = make_double2(0.0, 0.0);
+        if (!load_fused<KE, NL>(p, lane, tid, STHREADS, sM, sU, sMode, sRow, sS0, sF, &flag, sG, false)) {
+            for (int rho = tid; rho < p.m; rho += STHREADS) p.amp[lane * p.m + rho] = make_double2(0.0, 0.0);
             __syncthreads();
             continue;
         }
         const int64_t D = kk >= 1 ? ((int64_t)1 << (kk - 1)) : 1;
         int64_t t0, t1;
-        if (D >= THREADS) { const int64_t per = D / THREADS; t0 = tid * per; t1 = t0 + per; }
+        if (D >= STHREADS) { const int64_t per = D / STHREADS; t0 = tid * per; t1 = t0 + per; }
         else { t0 = tid; t1 = tid < D ? tid + 1 : tid; }
-        double2 acc[KE][NL];
-        walk<KE, NL>(sM, sU, k, t0, t1, sS0[0], sS0[1], make_double2(sF[0].x, -sF[0].y), make_double2(sF[1].x, -sF[1].y),
-                     acc);
-#pragma unroll
-        for (int j = 0; j < KE; ++j)
-#pragma unroll
-            for (int l = 0; l < NL; ++l) {
-                double2 x = acc[j][l];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    x.x += __shfl_xor_sync(0xffffffffu, x.x, o);
-                    x.y += __shfl_xor_sync(0xffffffffu, x.y, o);
-                }
-                if (lid == 0 && j < k) red[wid][j][l] = x;
-            }
+        walk_shared<KE, NL>(sM, sU, k, t0, t1, sS0[0], sS0[1], make_double2(sF[0].x, -sF[0].y),
+                            make_double2(sF[1].x, -sF[1].y), q, acc, tid, STHREADS);
         __syncthreads();
         const double norm = kk >= 1 ? ldexp(1.0, -(kk - 1)) : 1.0;
-        if (tid < k * NL) {
-            const int j = tid / NL, l = tid % NL;
+        if (tid < k * NL) {                                       // threads in order: deterministic
             double2 x = make_double2(0.0, 0.0);
-            for (int w = 0; w < NWARP; ++w) { x.x += red[w][j][l].x; x.y += red[w][j][l].y; }
-            sT[j][l] = make_double2(x.x * norm, x.y * norm);
+            for (int w = 0; w < STHREADS; ++w) { const double2 a = acc[tid * STHREADS + w]; x.x += a.x; x.y += a.y; }
+            sT[tid / NL][tid % NL] = make_double2(x.x * norm, x.y * norm);
         }
         __syncthreads();
-        for (int rho = tid; rho < p.m; rho += THREADS) {
+        for (int rho = tid; rho < p.m; rho += STHREADS) {
             double2 a = make_double2(0.0, 0.0);
             for (int c = 0; c < k; ++c)
 #pragma unroll
@@ -589,6 +664,24 @@ __global__ void __launch_bounds__(THREADS) emitter_step_kernel(StepParams p) {
         }
         __syncthreads();
     }
+}
+
+template <int KE, int NL>
+static int launch_step_wide(const StepParams& p, cudaStream_t st) {
+    const size_t dyn = step_dyn_smem<KE, NL>();
+    if (cudaFuncSetAttribute(emitter_step_kernel<KE, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) !=
+        cudaSuccess)
+        return PE_ERR_CUDA;
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emitter_step_kernel<KE, NL>, STHREADS, dyn) != cudaSuccess)
+        return PE_ERR_CUDA;
+    if (per < 1) return PE_ERR_SIZE;
+    int64_t grid = (int64_t)sms * per;
+    if (grid > p.nl) grid = p.nl;
+    emitter_step_kernel<KE, NL><<<(unsigned)grid, STHREADS, dyn, st>>>(p);
+    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
 }
 
 template <class K>
@@ -752,21 +845,11 @@ extern "C" int pe_emitter_step(const double* d_ut, int m, int M, const int64_t* 
                 emitter_step_warp_kernel<2><<<(unsigned)grid, 32 * WW, 0, st>>>(p);
             }
         } else if (k <= 16) {
-            if (L == 1) {
-                if ((rc = occupancy_grid(emitter_step_kernel<16, 1>, THREADS, nl, &grid)) != PE_OK) return rc;
-                emitter_step_kernel<16, 1><<<(unsigned)grid, THREADS, 0, st>>>(p);
-            } else {
-                if ((rc = occupancy_grid(emitter_step_kernel<16, 2>, THREADS, nl, &grid)) != PE_OK) return rc;
-                emitter_step_kernel<16, 2><<<(unsigned)grid, THREADS, 0, st>>>(p);
-            }
+            rc = L == 1 ? launch_step_wide<16, 1>(p, st) : launch_step_wide<16, 2>(p, st);
+            if (rc != PE_OK) return rc;
         } else {
-            if (L == 1) {
-                if ((rc = occupancy_grid(emitter_step_kernel<24, 1>, THREADS, nl, &grid)) != PE_OK) return rc;
-                emitter_step_kernel<24, 1><<<(unsigned)grid, THREADS, 0, st>>>(p);
-            } else {
-                if ((rc = occupancy_grid(emitter_step_kernel<24, 2>, THREADS, nl, &grid)) != PE_OK) return rc;
-                emitter_step_kernel<24, 2><<<(unsigned)grid, THREADS, 0, st>>>(p);
-            }
+            rc = L == 1 ? launch_step_wide<24, 1>(p, st) : launch_step_wide<24, 2>(p, st);
+            if (rc != PE_OK) return rc;
         }
         if (cudaGetLastError() != cudaSuccess) return PE_ERR_CUDA;
     }
