@@ -527,6 +527,142 @@ def run_emitter(args):
     print(json.dumps(line), flush=True)
 
 
+def run_latency_and_adaptive(args):
+    """`--config single`: one sample of the C2 workload (n = 20, m = 400) per fock_sample call — the latency
+    path (the reference's single.py: one stream spread over the GPU, here the split steps), ms per sample,
+    FP64 and mixed.  `--config adaptive`: the C2 workload with a forced prefix of 2 photons on modes (0, 1)
+    and those modes avoided afterwards (adaptive optics), 2 000 shots per call: surviving samples/s and
+    chains/s.  Both through the public fock_sample, U resident on the device."""
+    import torch
+
+    from photonic_engines_b200.clifford import fock_sample
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    g = torch.Generator().manual_seed(USEED)
+    z = torch.randn(M_MODES, M_MODES, generator=g, dtype=torch.float64) + 1j * torch.randn(
+        M_MODES, M_MODES, generator=g, dtype=torch.float64)
+    q, r = torch.linalg.qr(z)
+    d = torch.diagonal(r)
+    U = (q * (d / d.abs()).unsqueeze(0)).to(dev)
+    in_modes = list(range(N_PHOT))
+    out = {}
+    for precision in ("f64", "mixed"):
+        gen = torch.Generator(device=dev).manual_seed(11)
+        if args.config == "single":
+            kw, shots = {}, 1
+        else:
+            kw, shots = {"prefix": [0, 1], "avoid": [0, 1], "keep_ids": True}, SHOTS
+        for _ in range(args.warmup):
+            fock_sample(U, in_modes, shots, generator=gen, precision=precision, **kw)
+        torch.cuda.synchronize()
+        kept = 0
+        with ClockSampler(0) as clk:
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                res = fock_sample(U, in_modes, shots, generator=gen, precision=precision, **kw)
+                if args.config == "adaptive":
+                    kept += int(res[1].numel())
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+        if args.config == "single":
+            out[precision] = {"ms_per_sample": dt / args.steps * 1e3, "samples_per_s": args.steps / dt,
+                              "clocks": clk.summary()}
+        else:
+            out[precision] = {"chains_per_s": args.steps * shots / dt, "survivors_per_s": kept / dt,
+                              "survival": kept / (args.steps * shots), "ms_per_step": dt / args.steps * 1e3,
+                              "clocks": clk.summary()}
+    if args.config == "single":
+        line = {"config": "single", "workload": WORKLOAD.replace("2000 shots/step", "1 shot per call"),
+                "metric": "ms per sample (latency)", "unit": "ms", "value": out["f64"]["ms_per_sample"],
+                "higher_is_better": False, "fp64": out["f64"], "mixed": out["mixed"], "n_gpus": 1,
+                "steps": args.steps, "warmup": args.warmup, "data": "synthetic"}
+    else:
+        line = {"config": "adaptive", "workload": WORKLOAD + ", prefix (0, 1), avoid (0, 1)",
+                "metric": "surviving samples/s", "unit": "samples/s", "value": out["mixed"]["survivors_per_s"],
+                "higher_is_better": True, "fp64": out["f64"], "mixed": out["mixed"], "n_gpus": 1,
+                "steps": args.steps, "warmup": args.warmup, "data": "synthetic"}
+    print(json.dumps(line), flush=True)
+
+
+# The reference's published FP64 numbers on one H100 PCIe for workloads of this path (production
+# configuration): (label, n, m, shots per call, loss, published value, unit, source in the reference)
+PUBLISHED = [
+    ("s/sample n=24 m=2n", 24, 48, 2048, None, 0.35e-3, "s/sample", "docs/ALGORITHMS.md:186-194"),
+    ("s/sample n=28 m=2n", 28, 56, 256, None, 1.9e-3, "s/sample", "docs/ALGORITHMS.md:186-194"),
+    ("s/sample n=32 m=2n", 32, 64, 32, None, 22e-3, "s/sample", "docs/ALGORITHMS.md:186-194"),
+    ("samples/s k=20 m=24", 20, 24, 4096, None, 108.0e3, "samples/s", "results/keep/cost_table_20261011_h100.csv"),
+    ("samples/s k=20 m=32", 20, 32, 4096, None, 74.6e3, "samples/s", "results/keep/cost_table_20261011_h100.csv"),
+    ("samples/s k=20 m=48", 20, 48, 4096, None, 45.1e3, "samples/s", "results/keep/cost_table_20261011_h100.csv"),
+    ("samples/s k=20 m=96", 20, 96, 4096, None, 25.5e3, "samples/s", "results/keep/cost_table_20261011_h100.csv"),
+    ("samples/s k=28 m=96", 28, 96, 256, None, 248.0, "samples/s", "results/keep/cost_table_20261011_h100.csv"),
+    ("samples/s k=30 m=96", 30, 96, 64, None, 70.5, "samples/s", "results/keep/cost_table_20261011_h100.csv"),
+    ("samples/s n=27 m=324", 27, 324, 256, None, 178.0, "samples/s", "results/keep/frontier3_fock_r12_20260920_h100.csv"),
+    ("samples/s n=30 m=360", 30, 360, 64, None, 21.4, "samples/s", "results/keep/frontier3_fock_r12_20260920_h100.csv"),
+    ("ms/sample lossy n=24 m=48 eta=1", 24, 48, 4096, 1.0, 0.54, "ms/sample", "docs/LOSS.md:93-95"),
+    ("ms/sample lossy n=24 m=48 eta=0.9", 24, 48, 4096, 0.9, 0.22, "ms/sample", "docs/LOSS.md:93-95"),
+    ("ms/sample lossy n=24 m=48 eta=0.7", 24, 48, 4096, 0.7, 0.056, "ms/sample", "docs/LOSS.md:93-95"),
+    ("ms/sample lossy n=24 m=48 eta=0.5", 24, 48, 4096, 0.5, 0.034, "ms/sample", "docs/LOSS.md:93-95"),
+    ("ms/sample lossy n=20 m=40 eta=1", 20, 40, 4096, 1.0, 0.051, "ms/sample", "results/keep/bench_loss_h100.csv:10-17"),
+    ("ms/sample lossy n=20 m=40 eta=0.9", 20, 40, 4096, 0.9, 0.037, "ms/sample", "results/keep/bench_loss_h100.csv:10-17"),
+    ("ms/sample lossy n=20 m=40 eta=0.7", 20, 40, 4096, 0.7, 0.030, "ms/sample", "results/keep/bench_loss_h100.csv:10-17"),
+    ("ms/sample lossy n=20 m=40 eta=0.5", 20, 40, 4096, 0.5, 0.021, "ms/sample", "results/keep/bench_loss_h100.csv:10-17"),
+]
+PUBLISHED_ADDENDS = {24: 3.5e9, 28: 6.6e9, 32: 6.1e9}          # G addends/s, docs/ALGORITHMS.md:277-284
+
+
+def run_published(args):
+    """`--config published`: the workloads of the reference's published H100 numbers, run here through the
+    public fock_sample (FP64, photons in modes 0..n-1, seeded Haar U, CUDA generator), one line with this
+    GPU's figure, the published one and their ratio (> 1: faster here).  Frontier rows beyond 32 photons
+    (the compiled limit of this library) are not run."""
+    import numpy as np
+    import torch
+
+    from photonic_engines_b200.clifford import fock_sample
+    from photonic_engines_b200.clifford.work import chain_work
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rows_out = []
+    for label, n, m, shots, loss, pub, unit, src in PUBLISHED:
+        g = torch.Generator().manual_seed(1000 + n + m)
+        z = torch.randn(m, m, generator=g, dtype=torch.float64) + 1j * torch.randn(m, m, generator=g, dtype=torch.float64)
+        q, r = torch.linalg.qr(z)
+        d = torch.diagonal(r)
+        U = (q * (d / d.abs()).unsqueeze(0)).to(dev)
+        gen = torch.Generator(device=dev).manual_seed(5)
+        kw = {} if loss is None else {"loss": loss}
+        fock_sample(U, list(range(n)), shots, generator=gen, **kw)
+        torch.cuda.synchronize()
+        reps = max(1, args.steps // 2)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fock_sample(U, list(range(n)), shots, generator=gen, **kw)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / (reps * shots)               # seconds per sample
+        here = {"s/sample": dt, "ms/sample": dt * 1e3, "samples/s": 1.0 / dt}[unit]
+        ratio = pub / here if unit != "samples/s" else here / pub
+        row = {"workload": label, "n": n, "m": m, "shots": shots, "loss": loss, "here": here, "published_h100": pub,
+               "unit": unit, "speedup_vs_h100": ratio, "source": src}
+        if loss is None and n in PUBLISHED_ADDENDS and label.startswith("s/sample"):
+            # addends per sample from the rows of one call (the chain's exact term counts)
+            from photonic_engines_b200.clifford import sample_chains
+            sig = torch.argsort(torch.rand(min(shots, 64), n, generator=gen, device=dev), dim=1)
+            res = sample_chains(U, list(range(n)), sig, seeds=torch.randint(0, 2 ** 31 - 1, (n,), device=dev),
+                                split=None)
+            add = chain_work(res["rows"].cpu().numpy(), m)["addends"] / sig.shape[0]
+            row.update(addends_per_sample=add, g_addends_per_s=add / dt / 1e9,
+                       published_g_addends_per_s=PUBLISHED_ADDENDS[n] / 1e9)
+        rows_out.append(row)
+        print(json.dumps(row), file=sys.stderr, flush=True)
+    line = {"config": "published", "metric": "speed-up over the reference's published H100 numbers (same workloads)",
+            "unit": "x", "value": float(np.exp(np.mean([np.log(r_["speedup_vs_h100"]) for r_ in rows_out]))),
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic", "n_gpus": 1, "rows": rows_out,
+            "note": "geometric mean of the per-row ratios; frontier rows n = 34..40 exceed this library's 32 photons"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -535,8 +671,11 @@ def main():
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--ref-shots", type=int, default=0, help="chains per CPU sample (0: scaled to the cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--config", choices=("c1", "c2", "c3", "c4", "c5", "emitter"), default="c2",
-                    help="c2 (default) is the headline line; the others print one line through the batched sampler")
+    ap.add_argument("--config", choices=("c1", "c2", "c3", "c4", "c5", "emitter", "single", "adaptive", "published"),
+                    default="c2",
+                    help="c2 (default) is the headline line; c1 c3 c4 c5 run through the batched sampler, emitter "
+                         "the EmitterMPS path, single the one-sample latency path, adaptive prefix / avoid, published "
+                         "the workloads of the reference's published H100 numbers")
     ap.add_argument("--profile-launch", choices=("f64", "mixed"), default=None,
                     help="run only two chain launches of the workload (a target for ncu -s 1 -c 1)")
     args = ap.parse_args()
@@ -547,6 +686,12 @@ def main():
         args.warmup = 3
     if args.config == "emitter" and args.impl == "b200":
         run_emitter(args)
+        return
+    if args.config == "published" and args.impl == "b200":
+        run_published(args)
+        return
+    if args.config in ("single", "adaptive") and args.impl == "b200":
+        run_latency_and_adaptive(args)
         return
     if args.config != "c2" and args.impl == "b200":
         run_config(args)

@@ -22,7 +22,7 @@ from dataclasses import dataclass
 import torch
 
 from .. import _native as N
-from ..imperfections import partition, route_classical, spec
+from ..imperfections import draw_roles, partition, route_classical, spec
 from .kernels import chain, chain_adaptive, default_tpl, pack_instances, split_plan
 from .prefix import prefix_order
 
@@ -274,7 +274,8 @@ class ChainPlan:
     passes: list
 
 
-def plan_chains(U, in_modes, S: int, dp_all, generator, loss, indist, max_streams: int) -> ChainPlan:
+def plan_chains(U, in_modes, S: int, dp_all, generator, loss, indist, max_streams: int,
+                _force_general: bool = False) -> ChainPlan:
     """The chains of a call and every host-side draw, consuming `generator` as the reference does
     (sampler.py:146-215): lossless -> one pass of S streams; otherwise the partition on the host generator,
     one pass per surviving count k over the distinct column sets, singletons routed classically last."""
@@ -288,6 +289,8 @@ def plan_chains(U, in_modes, S: int, dp_all, generator, loss, indist, max_stream
         sig, seeds, chunk, off = _pass_draws(S, n, generator, dev, max_streams)
         return ChainPlan(S, n, S, dp_all, sig, None, seeds, chunk, off, None, None, None, None, [(n, S)])
     gen = _cpu_generator(generator)
+    if d is None and len(set(int(j) for j in in_modes)) == n and not _force_general:
+        return _plan_loss_only(U, in_modes, S, dp_all, generator, gen, loss, max_streams)
     by_cols: dict = {}                       # column tuple -> [stream ids]
     rep_sub: dict = {}                       # column tuple -> photon indices (columns of the packed instance)
     single_ids, single_cols = [], []
@@ -333,6 +336,76 @@ def plan_chains(U, in_modes, S: int, dp_all, generator, loss, indist, max_stream
     order = torch.argsort(nk.to(torch.int64), descending=True, stable=True)       # longest chains first
     return ChainPlan(S, n, int(nk.shape[0]), torch.cat(ch_dp), torch.cat(ch_cols), nk, torch.cat(all_seeds),
                      torch.cat(ch_row), torch.cat(ch_off), torch.cat(ch_out), order, s_ids, s_rows, passes)
+
+
+def _plan_loss_only(U, in_modes, S, dp_all, generator, gen, loss, max_streams) -> ChainPlan:
+    """plan_chains for uniform loss with distinct input modes, in tensor ops: the same role draws, passes,
+    stream order, per-pass draws and classical routing as the general loop.  A stream's group is its row of
+    roles among torch.unique's sorted rows; every group is one column set (its surviving photons), so the
+    passes are the groups' photon counts in order of first appearance, and within a pass the groups in
+    sorted order, each group's streams in ascending order; one-photon groups are routed classically."""
+    dev = U.device
+    n = len(in_modes)
+    roles = draw_roles(n, S, loss, None, generator=gen)
+    # rows hold LOST (0) or 2 only, so their lexicographic order (torch.unique over rows) is the order of
+    # the survival bitmask with photon 0 as the most significant bit: a 1-D unique gives the same groups
+    weights = torch.tensor([1 << (n - 1 - j) for j in range(n)], dtype=torch.int64)
+    mask = ((roles == 2).to(torch.int64) * weights).sum(1)
+    umask, inv = torch.unique(mask, return_inverse=True)
+    kept = ((umask[:, None] // weights[None, :]) % 2).bool()            # [G, n] surviving photons
+    kg = kept.sum(1)                                                     # photons per group
+    G = int(umask.shape[0])
+    multi = torch.nonzero(kg >= 2)[:, 0]
+    ks = []
+    for k in kg[multi].tolist():                                         # passes: first appearance
+        if k not in ks:
+            ks.append(k)
+    rank = torch.full((n + 1,), len(ks), dtype=torch.int64)
+    for r_, k in enumerate(ks):
+        rank[k] = r_
+    ch_dp, ch_cols, ch_nk, ch_row, ch_off, ch_out, all_seeds, passes = [], [], [], [], [], [], [], []
+    n_rows = 0
+    if ks:
+        key = rank[kg[inv]] * G + inv                                    # pass, then group; streams stable
+        key[kg[inv] < 2] = len(ks) * G + G                               # not in a pass
+        order_s = torch.sort(key, stable=True).indices
+        skey = key[order_s]
+        im = torch.as_tensor([int(j) for j in in_modes], dtype=torch.int64)
+        for r_, k in enumerate(ks):
+            sel = order_s[(skey >= r_ * G) & (skey < (r_ + 1) * G)]     # streams of this pass, in order
+            gsel = inv[sel]
+            groups_k, gidx = torch.unique_consecutive(gsel, return_inverse=True)
+            subs = torch.nonzero(kept[groups_k])[:, 1].reshape(-1, k).to(dev)        # [groups, k] photon ids
+            sig, seeds, chunk, off = _pass_draws(int(sel.shape[0]), k, generator, dev, max_streams)
+            ch_dp.append(dp_all[sel.to(dev)])
+            ch_cols.append(torch.nn.functional.pad(torch.gather(subs[gidx.to(dev)], 1, sig), (0, n - k)))
+            ch_nk.append(torch.full((sel.shape[0],), k, dtype=torch.int32, device=dev))
+            ch_row.append(chunk + n_rows)
+            ch_off.append(off)
+            ch_out.append(sel.to(dev))
+            all_seeds.append(torch.nn.functional.pad(seeds, (0, n - k)))
+            n_rows += seeds.shape[0]
+            passes.append((k, int(sel.shape[0])))
+    s_ids = s_rows = None
+    one = kg[inv] == 1
+    if bool(one.any()):
+        # streams of the one-photon groups, group by group in sorted order, ascending within a group
+        idx = torch.nonzero(one)[:, 0]
+        idx = idx[torch.sort(inv[idx], stable=True).indices]
+        photon = torch.nonzero(kept[inv[idx]])[:, 1]
+        s_ids = idx.to(dev)
+        s_rows = route_classical(U, dp_all[s_ids].cpu(), im_of(in_modes)[photon], generator=gen).to(dev)
+    if not ch_dp:
+        z = torch.zeros(0, dtype=torch.int64, device=dev)
+        return ChainPlan(S, n, 0, z, z.reshape(0, n), z.to(torch.int32), z.reshape(0, n), z, z, z, z, s_ids, s_rows, [])
+    nk = torch.cat(ch_nk)
+    order = torch.argsort(nk.to(torch.int64), descending=True, stable=True)
+    return ChainPlan(S, n, int(nk.shape[0]), torch.cat(ch_dp), torch.cat(ch_cols), nk, torch.cat(all_seeds),
+                     torch.cat(ch_row), torch.cat(ch_off), torch.cat(ch_out), order, s_ids, s_rows, passes)
+
+
+def im_of(in_modes) -> torch.Tensor:
+    return torch.as_tensor([int(j) for j in in_modes], dtype=torch.int64)
 
 
 def assemble_occupations(plan: ChainPlan, rows, m: int) -> torch.Tensor:

@@ -73,3 +73,23 @@ def test_loss_zero_transmission_returns_empty_samples():
                        None, 1 << 18)
     assert plan.C == 0 and plan.single_ids is None
     assert assemble_occupations(plan, None, 5).sum() == 0
+
+
+@pytest.mark.parametrize(("n", "m", "S", "eta", "in_modes", "B"), [
+    (20, 40, 1024, 0.5, list(range(20)), 1), (20, 40, 1024, 0.9, list(range(20)), 1),
+    (8, 12, 500, 0.3, [0, 2, 4, 6, 8, 9, 10, 11], 2), (6, 9, 300, 0.2, [5, 1, 3, 0, 8, 2], 1),
+    (32, 64, 200, 0.8, list(range(32)), 1)])
+def test_loss_only_plan_in_tensor_ops_is_the_general_plan(n, m, S, eta, in_modes, B):
+    """The vectorised plan for uniform loss (distinct input modes) makes the same draws and the same passes,
+    chains, order and classical routings as the reference-ordered loop over role groups."""
+    import torch
+    from oracle.oracle import haar_unitary
+    from photonic_engines_b200.clifford.sampler import plan_chains
+    U = torch.stack([torch.as_tensor(haar_unitary(m, 3 + b)) for b in range(B)])
+    dp = torch.arange(B).repeat_interleave(S // B)
+    a = plan_chains(U, in_modes, dp.shape[0], dp, torch.Generator().manual_seed(7), eta, None, 128)
+    b = plan_chains(U, in_modes, dp.shape[0], dp, torch.Generator().manual_seed(7), eta, None, 128, _force_general=True)
+    assert a.passes == b.passes and a.C == b.C
+    for f in ("dp", "cols", "nk", "seeds", "seed_row", "rng_off", "out_row", "order", "single_ids", "single_rows"):
+        x, y = getattr(a, f), getattr(b, f)
+        assert (x is None and y is None) or torch.equal(x, y), f
