@@ -260,6 +260,10 @@ int pe_read_status(const void* d_workspace, int* status, int64_t* detail, void* 
 /* Human-readable text of a status code. */
 const char* pe_status_string(int status);
 
+/* Text of the CUDA runtime error behind the calling thread's latest PE_ERR_CUDA return (no counterpart
+ * in the reference, whose Python wrappers raise the runtime's own exceptions). */
+const char* pe_last_cuda_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -92,6 +92,8 @@ def load() -> ctypes.CDLL:
     L.pe_read_status.argtypes = [_vp, ctypes.POINTER(_i32), ctypes.POINTER(_i64), _vp]
     L.pe_status_string.restype = ctypes.c_char_p
     L.pe_status_string.argtypes = [_i32]
+    L.pe_last_cuda_error.restype = ctypes.c_char_p
+    L.pe_last_cuda_error.argtypes = []
     _lib = L
     return L
 
@@ -102,12 +104,14 @@ EXPORTED = ("pe_version", "pe_max_modes", "pe_chain_workspace_bytes", "pe_fock_c
             "pe_fock_chain_adaptive", "pe_adaptive_workspace_bytes", "pe_emitter_weights",
             "pe_emitter_workspace_bytes", "pe_emitter_count", "pe_emitter_step",
             "pe_cofactors_rows", "pe_partition_shots", "pe_scatter_occupations", "pe_pipe_probe", "pe_read_status",
-            "pe_status_string")
+            "pe_status_string", "pe_last_cuda_error")
 
 
 def check(rc: int, what: str) -> None:
     if rc != PE_OK:
         msg = load().pe_status_string(rc).decode()
+        if rc == PE_ERR_CUDA:
+            msg += ": " + load().pe_last_cuda_error().decode()
         raise NativeError(f"{what}: status {rc} ({msg})")
 
 

@@ -16,9 +16,9 @@ WARP_CANDIDATES = [(1, 256), (2, 256)]          # the warp form: threads per lan
 CANDIDATES = {8: [(1, 128), (1, 256), (2, 128), (2, 256)],
               16: [(1, 128), (2, 128), (2, 256), (4, 256)],
               20: [(1, 128), (2, 128), (2, 256), (4, 128), (4, 256)],
-              24: [(2, 128), (2, 256), (4, 128), (4, 256)],
-              28: [(2, 256), (4, 128), (4, 256)],
-              32: [(2, 256), (4, 128), (4, 256)]}
+              24: [(2, 64), (2, 128), (4, 128), (4, 256)],
+              28: [(2, 64), (2, 128), (4, 128), (4, 256)],
+              32: [(2, 64), (2, 128), (4, 128), (4, 256)]}
 
 
 def _cache_path() -> str:
@@ -53,8 +53,13 @@ def tier(n: int) -> int:
     raise ValueError(f"at most 32 photons (got {n})")
 
 
+# bumped whenever the compiled launch shapes change, so that a cached choice the library no longer accepts
+# is never replayed
+SHAPES_VERSION = 2
+
+
 def key(device, precision: str, workload: str) -> str:
-    return f"{torch.cuda.get_device_name(device)}|{precision}|{workload}"
+    return f"v{SHAPES_VERSION}|{torch.cuda.get_device_name(device)}|{precision}|{workload}"
 
 
 def lookup(device, precision: str, workload: str):

@@ -73,7 +73,7 @@ def default_tpl(n: int, precision: str) -> int:
     kpm = next((k for k in (8, 16, 20, 24, 28, 32) if n <= k), 32)
     if kpm <= 8 or (precision == "f64" and kpm == 20):
         return 1
-    return 2 if kpm <= 24 else 4
+    return 2
 
 
 def split_plan(heavy_streams: int, n: int, device, block_threads: int = 0, tpl: int = 2):

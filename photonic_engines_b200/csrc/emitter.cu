@@ -14,6 +14,7 @@
 #include <stdint.h>
 
 #include "pe_b200.h"
+#include "pe_errors.h"
 
 namespace pe_em {
 
@@ -669,19 +670,16 @@ __global__ void __launch_bounds__(STHREADS) emitter_step_kernel(StepParams p) {
 template <int KE, int NL>
 static int launch_step_wide(const StepParams& p, cudaStream_t st) {
     const size_t dyn = step_dyn_smem<KE, NL>();
-    if (cudaFuncSetAttribute(emitter_step_kernel<KE, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) !=
-        cudaSuccess)
-        return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaFuncSetAttribute(emitter_step_kernel<KE, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emitter_step_kernel<KE, NL>, STHREADS, dyn) != cudaSuccess)
-        return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emitter_step_kernel<KE, NL>, STHREADS, dyn));
     if (per < 1) return PE_ERR_SIZE;
     int64_t grid = (int64_t)sms * per;
     if (grid > p.nl) grid = p.nl;
     emitter_step_kernel<KE, NL><<<(unsigned)grid, STHREADS, dyn, st>>>(p);
-    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+    return ::pe::launch_status();
 }
 
 template <class K>
@@ -689,7 +687,7 @@ static int occupancy_grid(K kernel, int threads, int64_t units, int64_t* grid) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0));
     if (per < 1) return PE_ERR_SIZE;
     *grid = (int64_t)sms * per;
     if (*grid > units) *grid = units;
@@ -702,14 +700,13 @@ static int launch_amp_warp(const Params& p, cudaStream_t st) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emitter_amp_warp_kernel<NL>, 32 * WW, 0) != cudaSuccess)
-        return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emitter_amp_warp_kernel<NL>, 32 * WW, 0));
     if (per < 1) return PE_ERR_SIZE;
     int64_t grid = (int64_t)sms * per;
     const int64_t need = (p.nl + WW - 1) / WW;
     if (grid > need) grid = need;
     emitter_amp_warp_kernel<NL><<<(unsigned)grid, 32 * WW, 0, st>>>(p);
-    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+    return ::pe::launch_status();
 }
 
 // w[s][rho] = sum over the stream's lanes lstart[s] .. lstart[s] + nlan[s] - 1, in order, of |amp|^2.
@@ -739,13 +736,12 @@ static int launch_amp(const Params& p, cudaStream_t st) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emitter_amp_kernel<KE, NL>, THREADS, 0) != cudaSuccess)
-        return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, emitter_amp_kernel<KE, NL>, THREADS, 0));
     if (per < 1) return PE_ERR_SIZE;
     int64_t grid = (int64_t)sms * per;
     if (grid > p.nl) grid = p.nl;
     emitter_amp_kernel<KE, NL><<<(unsigned)grid, THREADS, 0, st>>>(p);
-    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+    return ::pe::launch_status();
 }
 
 }  // namespace pe_em
@@ -768,7 +764,7 @@ extern "C" int pe_emitter_weights(const double* d_ut, int m, int M, const int64_
         return PE_ERR_ARG;
     if (workspace_bytes < 256) return PE_ERR_SIZE;
     cudaStream_t st = (cudaStream_t)stream;
-    if (cudaMemsetAsync(d_workspace, 0, 256, st) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, 256, st));
     if (S == 0) return PE_OK;
     Params p;
     p.UT = (const double2*)d_ut; p.m = m; p.M = M; p.rows = d_rows; p.rows_stride = rows_stride;
@@ -788,7 +784,7 @@ extern "C" int pe_emitter_weights(const double* d_ut, int m, int M, const int64_
     const int T = 256;
     emitter_weights_kernel<<<(unsigned)((total + T - 1) / T), T, 0, st>>>((const double2*)d_amp, d_lstart, d_nlan, S, m,
                                                                           nl, d_w, p.status, p.detail);
-    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+    return ::pe::launch_status();
 }
 
 extern "C" int pe_emitter_count(const int32_t* d_T, const int32_t* d_fid, int64_t S, int k, const int32_t* d_rg,
@@ -798,7 +794,7 @@ extern "C" int pe_emitter_count(const int32_t* d_T, const int32_t* d_fid, int64_
     if (!d_T || !d_fid || !d_rg || !d_r0 || !d_rf || !d_nlan || !d_workspace) return PE_ERR_ARG;
     if (workspace_bytes < 256) return PE_ERR_SIZE;
     cudaStream_t st = (cudaStream_t)stream;
-    if (cudaMemsetAsync(d_workspace, 0, 256, st) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, 256, st));
     if (S == 0) return PE_OK;
     StepParams p = {};
     p.T = d_T; p.fid = d_fid; p.S = S; p.k = k;
@@ -806,7 +802,7 @@ extern "C" int pe_emitter_count(const int32_t* d_T, const int32_t* d_fid, int64_
     p.status = (int*)((char*)d_workspace + 8);
     p.detail = (long long*)((char*)d_workspace + 16);
     emitter_count_kernel<<<(unsigned)((S + 255) / 256), 256, 0, st>>>(p, d_nlan);
-    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+    return ::pe::launch_status();
 }
 
 extern "C" int pe_emitter_step(const double* d_ut, int m, int M, const int64_t* d_rows, int rows_stride,
@@ -851,10 +847,10 @@ extern "C" int pe_emitter_step(const double* d_ut, int m, int M, const int64_t* 
             rc = L == 1 ? launch_step_wide<24, 1>(p, st) : launch_step_wide<24, 2>(p, st);
             if (rc != PE_OK) return rc;
         }
-        if (cudaGetLastError() != cudaSuccess) return PE_ERR_CUDA;
+        PE_CUDA_TRY(cudaGetLastError());
     }
     const int64_t total = S * (int64_t)m;
     emitter_weights_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>((const double2*)d_amp, d_lstart, d_nlan, S,
                                                                             m, nl, d_w, p.status, p.detail);
-    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+    return ::pe::launch_status();
 }

@@ -8,6 +8,7 @@
 #include "fock_kernels.cuh"
 #include "fock_registry.h"
 #include "fock_warp.cuh"
+#include "pe_errors.h"
 
 namespace pe {
 
@@ -26,7 +27,7 @@ static int kpm_index(int kpm) {
 static void* g_chain[2][3][N_KPM];
 static void* g_cof[2][3][N_KPM];
 static void* g_split_partial[2][3][N_KPM];
-static void* g_split_draw[2][N_KPM];
+static void* g_split_draw[2][3][N_KPM];
 static void* g_warp[2][3][N_KPM];
 
 void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cofactor_kernel, void* split_partial,
@@ -37,9 +38,7 @@ void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cof
     g_chain[mixed][ti][ki] = chain_kernel;
     g_cof[mixed][ti][ki] = cofactor_kernel;
     g_split_partial[mixed][ti][ki] = split_partial;
-    // the draw kernel does not depend on the lane width; keep one compiled for 256-thread CTAs (the
-    // one-thread-lane variants of 16 and 20 columns are compiled for 128)
-    if (!g_split_draw[mixed][ki] || tpl != 1) g_split_draw[mixed][ki] = split_draw;
+    g_split_draw[mixed][ti][ki] = split_draw;       // same launch bounds as the variant's other kernels
 }
 void* find_split_partial_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
@@ -50,9 +49,9 @@ void* find_warp_kernel(int mixed, int tpl, int kpm) {
     return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_warp[mixed][ti][ki];
 }
 size_t warp_smem_bytes() { return sizeof(WarpSmem) * WARPS; }
-void* find_split_draw_kernel(int mixed, int kpm) {
-    const int ki = kpm_index(kpm);
-    return (mixed < 0 || mixed > 1 || ki < 0) ? nullptr : g_split_draw[mixed][ki];
+void* find_split_draw_kernel(int mixed, int tpl, int kpm) {
+    const int ti = tpl_index(tpl), ki = kpm_index(kpm);
+    return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_split_draw[mixed][ti][ki];
 }
 void* find_chain_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
@@ -63,26 +62,36 @@ void* find_cofactor_kernel(int mixed, int tpl, int kpm) {
     return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_cof[mixed][ti][ki];
 }
 
-// Threads per Gray lane when the caller passes 0 (measured at m = 400, 2 000 streams): one-thread lanes
-// up to 8 columns, and for FP64 chains of 17-20 photons (no exchange of partial products; those variants
-// run 128-thread CTAs with 255 registers); two-thread lanes up to 24 columns, four beyond.
+// Threads per Gray lane when the caller passes 0 (measured at m = 400, 2 000 streams, and at m = 2n for
+// 21-32 photons): one-thread lanes up to 8 columns, and for FP64 chains of 17-20 photons (no exchange of
+// partial products; those variants run 128-thread CTAs with 255 registers); two-thread lanes beyond
+// (at 24-32 columns also compiled for 128-thread CTAs with 255 registers).
 static int default_tpl(int kpm, int precision) {
     if (kpm <= 8) return 1;
     if (precision == PE_PRECISION_F64 && kpm == 20) return 1;
-    return kpm <= 24 ? 2 : 4;
+    return 2;
 }
 
-// Largest CTA a compiled kernel accepts (its launch bounds).
+static thread_local cudaError_t g_last_cuda_error = cudaSuccess;
+
+int cuda_fail(cudaError_t e) {
+    g_last_cuda_error = e;
+    return PE_ERR_CUDA;
+}
+
+// Largest CTA a compiled kernel accepts (its launch bounds); 0 when the query fails (error recorded).
 static int max_block(void* fn) {
     cudaFuncAttributes a;
-    if (cudaFuncGetAttributes(&a, fn) != cudaSuccess) return 0;
+    const cudaError_t e = cudaFuncGetAttributes(&a, fn);
+    if (e != cudaSuccess) return cuda_fail(e), 0;
     return a.maxThreadsPerBlock;
 }
 
 static int max_smem_optin() {
     int dev = 0, v = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return cuda_fail(e), 0;
     return v;
 }
 
@@ -194,6 +203,10 @@ extern "C" size_t pe_chain_workspace_bytes(int64_t S) {
     return WS_BYTES;
 }
 
+extern "C" const char* pe_last_cuda_error(void) {
+    return g_last_cuda_error == cudaSuccess ? "no CUDA error recorded" : cudaGetErrorString(g_last_cuda_error);
+}
+
 extern "C" const char* pe_status_string(int status) {
     switch (status) {
         case PE_OK: return "ok";
@@ -210,18 +223,18 @@ extern "C" int pe_read_status(const void* d_workspace, int* status, int64_t* det
     int st = 0;
     long long det = 0;
     cudaStream_t s = (cudaStream_t)stream;
-    if (cudaMemcpyAsync(&st, (const char*)d_workspace + 8, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PE_ERR_CUDA;
-    if (cudaMemcpyAsync(&det, (const char*)d_workspace + 16, sizeof(long long), cudaMemcpyDeviceToHost, s) != cudaSuccess) return PE_ERR_CUDA;
-    if (cudaStreamSynchronize(s) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaMemcpyAsync(&st, (const char*)d_workspace + 8, sizeof(int), cudaMemcpyDeviceToHost, s));
+    PE_CUDA_TRY(cudaMemcpyAsync(&det, (const char*)d_workspace + 16, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    PE_CUDA_TRY(cudaStreamSynchronize(s));
     *status = st;
     if (detail) *detail = (int64_t)det;
     return PE_OK;
 }
 
 static int launch_prepare(void* fn, int block, size_t smem, int* grid_per_sm) {
-    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, smem) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, smem));
     if (occ < 1) return PE_ERR_SIZE;
     *grid_per_sm = occ;
     return PE_OK;
@@ -257,7 +270,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     if (warp_mode && (kpm > WMAXN || split)) return PE_ERR_SIZE;
     if (tpl == 0) {
         tpl = warp_mode ? (kpm <= 8 ? 1 : 2) : default_tpl(kpm, precision);
-        if (!warp_mode && !find_chain_kernel(precision, tpl, kpm)) tpl = kpm <= 24 ? 2 : 4;
+        if (!warp_mode && !find_chain_kernel(precision, tpl, kpm)) tpl = find_chain_kernel(precision, 2, kpm) ? 2 : 4;
     }
     if (tpl_index(tpl) < 0) return PE_ERR_ARG;
     void* fn = warp_mode ? find_warp_kernel(precision, tpl, kpm) : find_chain_kernel(precision, tpl, kpm);
@@ -273,8 +286,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     if (cap <= 0) return PE_ERR_CUDA;
     if (smem > (size_t)cap) return PE_ERR_SIZE;
     cudaStream_t st = (cudaStream_t)stream;
-    if (cudaMemsetAsync(d_workspace, 0, zero_status ? WS_BYTES : sizeof(unsigned long long), st) != cudaSuccess)
-        return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, zero_status ? WS_BYTES : sizeof(unsigned long long), st));
     if (S == 0) return PE_OK;
     const int klast = (k_last > 0 && k_last < n_stride) ? k_last : n_stride;
     int per_sm = 0;
@@ -301,12 +313,12 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     p.k_first = k_first;
     p.k_stop = split ? (k_split - 1 < klast ? k_split - 1 : klast) : (k_last > 0 ? klast : 0);
     void* args[] = {&p};
-    if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st));
     if (!split) return PE_OK;
     // the mixed form's guard band: flagged streams redo the step with the FP64 kernels (second pass)
     const int npass = precision == PE_PRECISION_MIXED ? 2 : 1;
     void* fpart[2] = {find_split_partial_kernel(precision, tpl, kpm), find_split_partial_kernel(PE_PRECISION_F64, tpl, kpm)};
-    void* fdraw[2] = {find_split_draw_kernel(precision, kpm), find_split_draw_kernel(PE_PRECISION_F64, kpm)};
+    void* fdraw[2] = {find_split_draw_kernel(precision, tpl, kpm), find_split_draw_kernel(PE_PRECISION_F64, tpl, kpm)};
     int64_t gpart[2], gdraw[2];
     const int64_t items = S * (int64_t)nch;
     for (int q = 0; q < npass; ++q) {
@@ -327,11 +339,8 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
         sp.k = k;
         for (int q = 0; q < npass; ++q) {
             sp.pass = q;
-            if (cudaLaunchKernel(fpart[q], dim3((unsigned)gpart[q]), dim3(block), sargs, smem_fixed_bytes(), st) !=
-                cudaSuccess)
-                return PE_ERR_CUDA;
-            if (cudaLaunchKernel(fdraw[q], dim3((unsigned)gdraw[q]), dim3(block), sargs, smem, st) != cudaSuccess)
-                return PE_ERR_CUDA;
+            PE_CUDA_TRY(cudaLaunchKernel(fpart[q], dim3((unsigned)gpart[q]), dim3(block), sargs, smem_fixed_bytes(), st));
+            PE_CUDA_TRY(cudaLaunchKernel(fdraw[q], dim3((unsigned)gdraw[q]), dim3(block), sargs, smem, st));
         }
     }
     return PE_OK;
@@ -400,8 +409,7 @@ extern "C" int pe_fock_chain_adaptive(int precision, const double* d_acol, const
     const int ks = (k_split > 0 && k_split <= n_stride) ? k_split : 0;
     const bool warp = mode == 1;
     if (!d_avoid || n_prefix == n_stride) {
-        if (d_alive && S > 0 && cudaMemsetAsync(d_alive, 1, (size_t)S, (cudaStream_t)stream) != cudaSuccess)
-            return PE_ERR_CUDA;
+        if (d_alive && S > 0) PE_CUDA_TRY(cudaMemsetAsync(d_alive, 1, (size_t)S, (cudaStream_t)stream));
         return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, nullptr, d_cols,
                             n_stride, d_uniforms, d_seeds, d_seed_row, d_rng_off, nullptr, d_rows, d_occ, occ_stride,
                             nullptr, m_max, d_workspace, workspace_bytes, block_threads, tpl, 0, ks, nch, stream, warp,
@@ -421,13 +429,13 @@ extern "C" int pe_fock_chain_adaptive(int precision, const double* d_acol, const
     a.status = (int*)(w + 8);
     a.detail = (long long*)(w + 16);
     cudaStream_t st = (cudaStream_t)stream;
-    if (cudaMemsetAsync(d_workspace, 0, WS_BYTES, st) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, WS_BYTES, st));
     if (S == 0) return PE_OK;
     for (int k = n_prefix + 1; k <= n_stride; ++k) {
         a.col = k == n_prefix + 1 ? -1 : k - 2;            // no check before the first free step
         a.zero_dead = 0;
         avoid_update_kernel<<<1, 1024, 0, st>>>(a);
-        if (cudaGetLastError() != cudaSuccess) return PE_ERR_CUDA;
+        PE_CUDA_TRY(cudaGetLastError());
         const int rc = chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, a.nk,
                                     d_cols, n_stride, d_uniforms, d_seeds, d_seed_row, a.rng, nullptr, d_rows,
                                     k == n_stride ? d_occ : nullptr, occ_stride, nullptr, m_max, d_workspace,
@@ -437,7 +445,7 @@ extern "C" int pe_fock_chain_adaptive(int precision, const double* d_acol, const
     a.col = n_stride - 1;                                 // the last photon is checked too
     a.zero_dead = 1;
     avoid_update_kernel<<<1, 1024, 0, st>>>(a);
-    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+    return ::pe::launch_status();
 }
 
 extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t* d_rows, int64_t S, int m, int K,
@@ -449,14 +457,16 @@ extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t
     if (workspace_bytes < WS_BYTES || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
     const int kpm = kpm_for(K);
     if (kpm < 0) return PE_ERR_SIZE;
-    if (tpl == 0) tpl = kpm <= 8 ? 1 : (kpm <= 24 ? 2 : 4);
+    if (tpl == 0) tpl = kpm <= 8 ? 1 : 2;
     if (tpl_index(tpl) < 0) return PE_ERR_ARG;
     void* fn = find_cofactor_kernel(precision, tpl, kpm);
     if (!fn) return PE_ERR_SIZE;
-    const int block = block_threads ? block_threads : 256;
-    if (block < 32 || block > 256 || (block & 31)) return PE_ERR_ARG;
+    const int bmax = max_block(fn);
+    if (bmax < 32) return PE_ERR_CUDA;
+    const int block = block_threads ? block_threads : (bmax < 256 ? bmax : 256);
+    if (block < 32 || block > 256 || block > bmax || (block & 31)) return PE_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    if (cudaMemsetAsync(d_workspace, 0, WS_BYTES, st) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, WS_BYTES, st));
     if (S == 0) return PE_OK;
     const size_t smem = smem_fixed_bytes();
     int per_sm = 0;
@@ -472,7 +482,7 @@ extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t
     int* status = (int*)((char*)d_workspace + 8);
     long long* detail = (long long*)((char*)d_workspace + 16);
     void* args[] = {(void*)&a, (void*)&d_rows, (void*)&S, (void*)&m, (void*)&K, (void*)&pp, (void*)&status, (void*)&detail};
-    if (cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st));
     return PE_OK;
 }
 
@@ -480,8 +490,8 @@ extern "C" int pe_pipe_probe(int precision, int iters, void* d_out, size_t out_b
     if ((precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) || iters < 1 || !d_out || !flops)
         return PE_ERR_ARG;
     int dev = 0, sms = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return PE_ERR_CUDA;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaGetDevice(&dev));
+    PE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int threads = 256, blocks = sms * 8;
     const size_t need = (size_t)blocks * threads * (precision == PE_PRECISION_F64 ? 8 : 4);
     if (out_bytes < need) return PE_ERR_SIZE;
@@ -490,7 +500,7 @@ extern "C" int pe_pipe_probe(int precision, int iters, void* d_out, size_t out_b
         pipe_probe_kernel<double><<<blocks, threads, 0, st>>>((double*)d_out, 0.999999, 1e-7, iters);
     else
         pipe_probe_kernel<float><<<blocks, threads, 0, st>>>((float*)d_out, 0.999999f, 1e-7f, iters);
-    if (cudaGetLastError() != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaGetLastError());
     *flops = 2.0 * 8.0 * (double)iters * (double)blocks * (double)threads;
     return PE_OK;
 }
@@ -518,7 +528,7 @@ static std::mutex g_noalloc_mutex;
 // stand-in; the address comes from cudaGetSymbolAddress, once per device, with that device current.
 static int noalloc_scratch(void** out) {
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= PE_NOALLOC_MAX_DEVICES) return PE_ERR_SIZE;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
     if (!g_noalloc_ptr[dev]) {
@@ -546,8 +556,8 @@ extern "C" int pe_fock_chain_noalloc(int precision, const double* d_acol, const 
                                  occ_stride, d_marg, marg_stride, scratch, PE_NOALLOC_SCRATCH_BYTES, block_threads, tpl,
                                  grid_ctas, stream);
     if (rc != PE_OK) return rc;
-    if (d_status && cudaMemcpyAsync(d_status, (const char*)scratch + 8, sizeof(int), cudaMemcpyDeviceToDevice,
-                                    (cudaStream_t)stream) != cudaSuccess)
-        return PE_ERR_CUDA;
+    if (d_status)
+        PE_CUDA_TRY(cudaMemcpyAsync(d_status, (const char*)scratch + 8, sizeof(int), cudaMemcpyDeviceToDevice,
+                                    (cudaStream_t)stream));
     return PE_OK;
 }

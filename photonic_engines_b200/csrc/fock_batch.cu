@@ -12,6 +12,7 @@
 
 #include "pe_b200.h"
 #include "pe_device.cuh"
+#include "pe_errors.h"
 
 namespace pe {
 
@@ -108,7 +109,7 @@ extern "C" int pe_partition_shots(const int64_t* d_dp, const int32_t* d_inst_n, 
     const int threads = 128;
     partition_kernel<<<(unsigned)((S + threads - 1) / threads), threads, 0, (cudaStream_t)stream>>>(
         d_dp, d_inst_n, d_eta, d_x, S, n_stride, singles, d_key, d_cols, d_nk, d_chain_dp, d_out_row, d_status);
-    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+    return ::pe::launch_status();
 }
 
 extern "C" int pe_scatter_occupations(const int64_t* d_rows, const int32_t* d_nk, const int64_t* d_out_row, int64_t C,
@@ -117,10 +118,10 @@ extern "C" int pe_scatter_occupations(const int64_t* d_rows, const int32_t* d_nk
     if (C < 0 || S < 0 || n_stride < 1 || occ_stride < 1 || !d_rows || !d_nk || !d_out_row || !d_occ || !d_status)
         return PE_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
-    if (cudaMemsetAsync(d_occ, 0, (size_t)S * occ_stride * sizeof(int64_t), st) != cudaSuccess) return PE_ERR_CUDA;
+    PE_CUDA_TRY(cudaMemsetAsync(d_occ, 0, (size_t)S * occ_stride * sizeof(int64_t), st));
     if (C == 0) return PE_OK;
     const int threads = 128;
     scatter_occ_kernel<<<(unsigned)((C + threads - 1) / threads), threads, 0, st>>>(d_rows, d_nk, d_out_row, C, n_stride,
                                                                                    d_occ, occ_stride, S, d_status);
-    return cudaGetLastError() == cudaSuccess ? PE_OK : PE_ERR_CUDA;
+    return ::pe::launch_status();
 }

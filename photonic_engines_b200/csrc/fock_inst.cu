@@ -16,7 +16,7 @@ struct Registration {
                              (void*)pe::fock_chain_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
                              (void*)pe::cofactor_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
                              (void*)pe::split_partial_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
-                             (void*)pe::split_draw_kernel<PE_KPM, (PE_MIXED != 0)>,
+                             (void*)pe::split_draw_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
 #if PE_KPM <= 16 && PE_TPL <= 2
                              (void*)pe::fock_chain_warp_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>
 #else

@@ -1105,7 +1105,9 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_partial_kernel(SplitPa
     }
 }
 
-template <int KPM, bool MIXED>
+// TPL does not enter the draw; it keeps the kernel's symbol distinct in every variant object, whose
+// launch bounds differ (one shared symbol would let the runtime launch any object's copy).
+template <int TPL, int KPM, bool MIXED>
 __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_draw_kernel(SplitParams sp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& sm = *reinterpret_cast<Smem*>(smem_raw);

@@ -9,7 +9,7 @@ void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cof
 void* find_chain_kernel(int mixed, int tpl, int kpm);
 void* find_cofactor_kernel(int mixed, int tpl, int kpm);
 void* find_split_partial_kernel(int mixed, int tpl, int kpm);
-void* find_split_draw_kernel(int mixed, int kpm);
+void* find_split_draw_kernel(int mixed, int tpl, int kpm);
 void* find_warp_kernel(int mixed, int tpl, int kpm);
 size_t warp_smem_bytes();
 

@@ -28,3 +28,4 @@ def test_loader_sets_signatures_and_version():
     assert L.pe_version() >= 100
     assert L.pe_chain_workspace_bytes(1000) >= 64
     assert L.pe_status_string(-2).decode().startswith("size")
+    assert L.pe_last_cuda_error().decode() == "no CUDA error recorded"     # no CUDA call has failed

@@ -1,11 +1,13 @@
 """Parity of the CUDA path (through the C ABI) with the oracle and with the reference's recorded draws.
 
-Tolerances: FP64 form — cofactors and marginals within 1e-10 relative (normwise), picks bit-exact;
+Tolerances: FP64 form — cofactors and marginals within 1e-10 relative (normwise) up to 24 columns,
+growing 1.8x per column beyond (f64_tol), picks bit-exact;
 mixed form — picks identical to the FP64 form's (the guard band sends ambiguous draws through the FP64
 sweep), cofactors and marginals within the FP32 envelope mixed_tol(k) = 2e-7 * 1.35^k (about 1e-6 at
 k = 10, 8e-5 at k = 20; the measured maxima sit 2-4x below it).  A pick is compared whenever the oracle's
 draw lies farther than 1e-11 * total weight from every CDF step (closer draws are counted and must be
 rare)."""
+import functools
 import math
 import os
 
@@ -157,6 +159,43 @@ def test_chains_match_the_oracle_with_supplied_uniforms(n, m, S, mode):
             assert _rel(mmx[s, k], ref["marg"][s, k]) <= mixed_tol(k + 1)
 
 
+def f64_tol(k: int) -> float:
+    """FP64 envelope at a step with k columns: 1e-10 up to 24, growing 1.8x per column beyond (sums of
+    2^(k-2) terms; the FP64 oracle itself sits 1.9e-10 from its long-double form at k = 29)."""
+    return F64_TOL * max(1.0, 1.8 ** (k - 24))
+
+
+@functools.lru_cache(maxsize=None)
+def _long_chain_case(n):
+    """Three chains of n photons in m = 2n modes and the long-double oracle's rows, gaps and marginals."""
+    m, S = 2 * n, 3
+    U, sig, u = _random_chains(n, m, S, 500 + n)
+    return U, sig, u, O.chain(U[:, :n], np.zeros(S, np.int64), sig, u, precision="ld", marg=True, threads=S)
+
+
+@pytest.mark.parametrize("tpl", [0, 4])
+@pytest.mark.parametrize("n", [22, 26, 29])
+def test_long_chains_match_the_oracle_at_the_wide_tiers(n, tpl):
+    """Chains of 22, 26 and 29 photons (the 24-, 28- and 32-column kernels) in the default two-thread
+    lanes and in four-thread lanes, heavy steps split over the GPU, against the long-double oracle: FP64
+    picks bit-exact and marginals within f64_tol(k); mixed picks equal to the FP64 picks, marginals within
+    mixed_tol(k)."""
+    U, sig, u, ref = _long_chain_case(n)
+    Ut = torch.tensor(U, device=DEV)
+    f64 = sample_chains(Ut, list(range(n)), sig, uniforms=u, want_marg=True, tpl=tpl, split=None)
+    mix = sample_chains(Ut, list(range(n)), sig, uniforms=u, want_marg=True, tpl=tpl, split=None, precision="mixed")
+    rows64 = f64["rows"].cpu().numpy()
+    far = (ref["gap"] > 1e-11).all(axis=1)
+    assert far.sum() >= 2
+    assert np.array_equal(rows64[far], ref["rows"][far])
+    assert np.array_equal(mix["rows"].cpu().numpy(), rows64)
+    m64, mmx = f64["marg"].cpu().numpy(), mix["marg"].cpu().numpy()
+    for s in np.nonzero(far)[0]:
+        for k in range(n):
+            assert _rel(m64[s, k], ref["marg"][s, k]) <= f64_tol(k + 1), (s, k)
+            assert _rel(mmx[s, k], ref["marg"][s, k]) <= mixed_tol(k + 1), (s, k)
+
+
 @pytest.mark.parametrize("block,tpl", CONFIGS)
 def test_launch_shapes_give_identical_picks(block, tpl):
     n, m, S = 10, 30, 40
@@ -279,6 +318,25 @@ def test_split_steps_match_single_cta_chains(precision, k_split, nch):
         for k in range(n):
             tol = 1e-12 if precision == "f64" else mixed_tol(k + 1)      # FP32 blocks start at other lanes
             assert _rel(mb[s, k], ma[s, k]) <= tol
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+@pytest.mark.parametrize("n,shapes", [(18, [(1, 128), (2, 256), (4, 256), (1, 64)]),
+                                      (22, [(2, 128), (2, 64), (4, 256), (4, 128), (2, 128)])])
+def test_split_steps_in_every_launch_shape_one_after_another(precision, n, shapes):
+    """Split steps in launch shapes of variants compiled for 128- and 256-thread CTAs, in one process and
+    in turn (an autotuner's order): each variant launches its own draw kernel, every shape gives the same
+    picks."""
+    m, S = 2 * n, 4
+    U, sig, u = _random_chains(n, m, S, 71 + n)
+    Ut = torch.tensor(U, device=DEV)
+    first = None
+    for tpl, block in shapes:
+        out = sample_chains(Ut, list(range(n)), sig, uniforms=u, precision=precision, split=(12, 4), tpl=tpl,
+                            block_threads=block)
+        rows = out["rows"].cpu().numpy()
+        first = rows if first is None else first
+        assert np.array_equal(rows, first), (tpl, block)
 
 
 def test_single_sample_uses_the_whole_gpu_and_matches_the_oracle():
