@@ -119,6 +119,13 @@ int pe_fock_chain_warp(int precision, const double* d_acol, const int64_t* d_ins
 /* Bytes of device workspace pe_fock_chain_split needs for S streams and nch CTAs per stream. */
 size_t pe_chain_split_workspace_bytes(int64_t S, int nch);
 
+/* CTAs of the split-step kernel resident at once on the current device (SMs x CTAs per SM) for chains
+ * of n_stride photons in the given precision, CTA size and lane width (0: the defaults of
+ * pe_fock_chain_split); a negative status on bad arguments.  Callers size nch with it: S * nch a
+ * little under a multiple of it, nch a power of two (the Gray lanes of a step come in powers of two).
+ * Replaces the lane-grid sizing of photonic_engines/clifford/cofactors_triton.py:450-465. */
+int pe_split_slots(int precision, int n_stride, int block_threads, int tpl);
+
 /*
  * Adaptive chains: a forced prefix and an avoided set of output modes (photonic_engines/clifford/
  * sampler.py:391-460, `_sample_streams(..., prefix=, avoid=)`, reached from fock_sample(prefix=, avoid=),

@@ -94,13 +94,15 @@ def load() -> ctypes.CDLL:
     L.pe_status_string.argtypes = [_i32]
     L.pe_last_cuda_error.restype = ctypes.c_char_p
     L.pe_last_cuda_error.argtypes = []
+    L.pe_split_slots.restype = _i32
+    L.pe_split_slots.argtypes = [_i32, _i32, _i32, _i32]
     _lib = L
     return L
 
 
 # every symbol the C header declares (checked by the CPU test that loads the library)
 EXPORTED = ("pe_version", "pe_max_modes", "pe_chain_workspace_bytes", "pe_fock_chain", "pe_fock_chain_noalloc",
-            "pe_fock_chain_split", "pe_chain_split_workspace_bytes", "pe_fock_chain_warp",
+            "pe_fock_chain_split", "pe_chain_split_workspace_bytes", "pe_split_slots", "pe_fock_chain_warp",
             "pe_fock_chain_adaptive", "pe_adaptive_workspace_bytes", "pe_emitter_weights",
             "pe_emitter_workspace_bytes", "pe_emitter_count", "pe_emitter_step",
             "pe_cofactors_rows", "pe_partition_shots", "pe_scatter_occupations", "pe_pipe_probe", "pe_read_status",

@@ -95,7 +95,7 @@ class BatchedSampler:
         self.status = torch.zeros(2, dtype=torch.int32, device=dev)
         self.warp = use_warp_form(self.S, self.n_stride, dev)           # short chains: one warp per stream
         self.split = None if self.warp else split_plan(self.S, self.n_stride, dev, 0,           # few long chains
-                                                        default_tpl(self.n_stride, precision))
+                                                        default_tpl(self.n_stride, precision), precision)
         if self.split:
             self.ws = torch.empty(int(N.load().pe_chain_split_workspace_bytes(C, self.split[1])), dtype=torch.uint8,
                                   device=dev)

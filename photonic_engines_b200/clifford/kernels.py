@@ -9,6 +9,8 @@ All tensors are CUDA tensors; launches go on torch's current stream of that devi
 """
 from __future__ import annotations
 
+import functools
+
 import torch
 
 from .. import _native as N
@@ -76,16 +78,50 @@ def default_tpl(n: int, precision: str) -> int:
     return 2
 
 
-def split_plan(heavy_streams: int, n: int, device, block_threads: int = 0, tpl: int = 2):
+NCH_MAX = 64                 # CTAs per stream at most
+
+
+@functools.lru_cache(maxsize=None)
+def _split_slots(device_index: int, precision: str, n: int, block_threads: int, tpl: int) -> int:
+    L = N.load()
+    with torch.cuda.device(device_index):
+        slots = int(L.pe_split_slots(N.PRECISIONS[precision], n, block_threads, tpl))
+    N.check(min(slots, 0), "pe_split_slots")
+    return slots
+
+
+def split_plan(heavy_streams: int, n: int, device, block_threads: int = 0, tpl: int = 2, precision: str = "f64"):
     """(k_split, nch) for a batch whose long chains number `heavy_streams`, or None when one CTA per stream
-    already fills the GPU.  nch CTAs share every step k >= k_split of a stream; k_split is the first step
-    with enough Gray terms (2^(k-2)) for every CTA to run several lanes."""
-    block = block_threads or DEFAULT_BLOCK
-    slots = torch.cuda.get_device_properties(device).multi_processor_count * max(1, 512 // block)
-    if heavy_streams >= slots or n < 8:
+    already fills the GPU several times over.  nch CTAs share every step k >= k_split of a stream.
+
+    nch is a power of two (a step's Gray lanes come in powers of two, so any other count leaves lanes idle)
+    with heavy_streams * nch at least six times the split kernel's resident CTAs (`pe_split_slots`), so
+    that the last partial wave costs little (at most 64); of nch and 2 nch the one that fills its waves
+    better (by more than 2 %) wins.  k_split is the first step with enough Gray terms (2^(k-2)) for every
+    CTA to run several lanes.  The reference's single-sample path sizes a fixed lane grid instead
+    (photonic_engines/clifford/single.py:22-82)."""
+    if n < 8 or heavy_streams < 1:
         return None
-    nch = min(64, -(-2 * slots // max(heavy_streams, 1)))
+    dev = torch.device(device)
+    block = block_threads or DEFAULT_BLOCK
+    tpl = tpl or default_tpl(n, precision)
+    slots = _split_slots(dev.index if dev.index is not None else torch.cuda.current_device(), precision, n,
+                         block, tpl)
+    if heavy_streams >= 3 * slots:
+        return None
+
+    def fill(c):
+        items = heavy_streams * c
+        return items / (-(-items // slots) * slots)
+
+    nch = 1
+    while nch < NCH_MAX and heavy_streams * nch < 6 * slots:
+        nch *= 2
+    if 2 * nch <= NCH_MAX and fill(2 * nch) > fill(nch) + 0.02:
+        nch *= 2
     lanes = block // max(tpl, 1)
+    while nch > 1 and (1 << (n - 2)) < 4 * nch * lanes:      # the last step must still be split
+        nch //= 2
     k = 2
     while k <= n and (1 << (k - 2)) < 4 * nch * lanes:
         k += 1

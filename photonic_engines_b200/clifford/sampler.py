@@ -79,7 +79,7 @@ def sample_chains(U, in_modes, sigma, *, uniforms=None, seeds=None, seed_row=Non
         dp = torch.zeros(S, dtype=torch.int64, device=dev)
     acol, inst_off, inst_m, inst_n = pack_instances(U, in_modes)
     if split is None:
-        split = split_plan(S, n, dev, block_threads, tpl or default_tpl(n, precision))
+        split = split_plan(S, n, dev, block_threads, tpl or default_tpl(n, precision), precision)
     rows, occ, marg = chain(acol, inst_off, inst_m, inst_n, dp, sigma, uniforms=uniforms, seeds=seeds,
                             seed_row=seed_row, rng_off=rng_off, want_occ=True, want_marg=want_marg,
                             precision=precision, block_threads=block_threads, tpl=tpl, grid_ctas=grid_ctas,
@@ -186,7 +186,8 @@ def fock_sample(U, in_modes, shots, generator=None, algo="auto", multi_min_k1=10
         rows, occ_k, _ = chain(acol, inst_off, inst_m, inst_n, plan.dp, plan.cols, m_max=m, nk=plan.nk, uniforms=u,
                                seeds=plan.seeds, seed_row=plan.seed_row, rng_off=plan.rng_off, order=plan.order,
                                want_occ=direct, precision=precision, block_threads=block_threads, tpl=tpl,
-                               split=split_plan(heavy, n, dev, block_threads, tpl or default_tpl(n, precision)))
+                               split=split_plan(heavy, n, dev, block_threads,
+                                                tpl or default_tpl(n, precision), precision))
         if direct:
             occ = occ_k
     if stats is not None:
@@ -239,7 +240,8 @@ def _adaptive(U, in_modes, S, dp_all, generator, max_streams, prefix, avoid, kee
     _, occ, alive = chain_adaptive(acol, inst_off, inst_m, inst_n, dp_all, torch.cat(sig), rows, c0, m_max=m,
                                    avoid=mask, uniforms=u, seeds=torch.stack(seeds), seed_row=torch.cat(chunk),
                                    rng_off=torch.cat(off), precision=precision, block_threads=block_threads, tpl=tpl,
-                                   split=split_plan(S, n, dev, block_threads, tpl or default_tpl(n, precision)))
+                                   split=split_plan(S, n, dev, block_threads,
+                                                    tpl or default_tpl(n, precision), precision))
     if stats is not None:
         torch.cuda.synchronize(dev)
         stats["fused_seconds"] = _time.perf_counter() - t0

@@ -486,6 +486,29 @@ extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t
     return PE_OK;
 }
 
+extern "C" int pe_split_slots(int precision, int n_stride, int block_threads, int tpl) {
+    if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
+    const int kpm = kpm_for(n_stride);
+    if (n_stride < 1 || kpm < 0) return PE_ERR_SIZE;
+    if (tpl == 0) {
+        tpl = default_tpl(kpm, precision);
+        if (!find_chain_kernel(precision, tpl, kpm)) tpl = find_chain_kernel(precision, 2, kpm) ? 2 : 4;
+    }
+    if (tpl_index(tpl) < 0) return PE_ERR_ARG;
+    void* fn = find_split_partial_kernel(precision, tpl, kpm);
+    if (!fn) return PE_ERR_SIZE;
+    const int bmax = max_block(fn);
+    if (bmax < 32) return PE_ERR_CUDA;
+    const int block = block_threads ? block_threads : (bmax < 128 ? bmax : 128);
+    if (block < 32 || block > 256 || block > bmax || (block & 31)) return PE_ERR_ARG;
+    int per_sm = 0, dev = 0, sms = 0;
+    const int rc = launch_prepare(fn, block, smem_fixed_bytes(), &per_sm);
+    if (rc != PE_OK) return rc;
+    PE_CUDA_TRY(cudaGetDevice(&dev));
+    PE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return sms * per_sm;
+}
+
 extern "C" int pe_pipe_probe(int precision, int iters, void* d_out, size_t out_bytes, double* flops, void* stream) {
     if ((precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) || iters < 1 || !d_out || !flops)
         return PE_ERR_ARG;
