@@ -104,6 +104,25 @@ __device__ __forceinline__ void add_to_groups(SM& sm, int row) {
     sm.ngrp += 1;
 }
 
+// One whole warp: the groups of sm.rows[0, count) (count <= 32) in order of first appearance, as
+// `count` calls of add_to_groups would leave them, in a few warp instructions: the lanes holding the
+// same row find each other (match), the lowest of them leads, and leaders are numbered in lane order.
+template <class SM>
+__device__ __forceinline__ void build_groups_warp(SM& sm, int count) {
+    const int lane = threadIdx.x & 31;
+    const bool has = lane < count;
+    const int row = has ? sm.rows[lane] : -1 - lane;          // absent lanes: distinct non-rows
+    const unsigned same = __match_any_sync(0xffffffffu, row);
+    const bool leader = has && (__ffs(same) - 1 == lane);
+    const unsigned leaders = __ballot_sync(0xffffffffu, leader);
+    if (leader) {
+        const int g = __popc(leaders & ((1u << lane) - 1u));
+        sm.grow[g] = row;
+        sm.gmul[g] = __popc(same);
+    }
+    if (lane == 0) sm.ngrp = __popc(leaders);
+}
+
 // ---------------------------------------------------------------------------------------- plan
 // Warp 0.  Lane g holds group g.  Radix = mult + 1, and one odd-multiplicity group (the last one)
 // has its radix halved to (mult + 1) / 2 with the scale doubled — the complement symmetry
@@ -204,7 +223,23 @@ __device__ void plan_step(SM& sm, int K1, int K, int lanes, int lin_max, int mid
 // `d0` with radices R and prefix products Pp: its weight prod (-1)^v C(M, v) and the transition
 // into it (the digit the odometer moved, and the sign of the column-sum update -2 dir b).
 static __device__ __forceinline__ unsigned char gray_entry(const Plan& pl, int d0, int nd, const int* Pp, int t,
-                                                          double* w_out, unsigned char* vend) {
+                                                          double* w_out, unsigned char* vend, bool binary) {
+    if (binary) {                                   // every radix 2: the digits are the bits of t
+        const int qstar = t > 0 ? __ffs(t) - 1 : -1;
+        int par = 0, parh = 0;
+        double w = 1.0;
+        for (int q = nd - 1; q >= 0; --q) {
+            if (q == qstar) parh = par;
+            const int d = (t >> q) & 1;
+            const int v = (par & 1) ? 1 - d : d;
+            if (vend) vend[q] = (unsigned char)v;
+            par += v;
+            if (v) w *= -(double)pl.M[d0 + q];      // (-1)^v C(M, v) at v = 1
+        }
+        *w_out = w;
+        if (qstar < 0) return 0;
+        return (unsigned char)(qstar | ((parh & 1) ? 0 : 0x80));
+    }
     int qstar = -1;
     if (t > 0) {
         for (int q = 0; q < nd; ++q)
@@ -254,15 +289,18 @@ static __device__ void prepare_step(Smem& sm, const double2* __restrict__ A, int
                 make_float4((float)(2.0 * b1.x), (float)(2.0 * b2.x), (float)(2.0 * b1.y), (float)(2.0 * b2.y));
         }
     }
+    bool bin_in = true, bin_mid = true;             // schedules of radix-2 digits only (distinct rows)
+    for (int q = 0; q < pl.nin; ++q) bin_in = bin_in && pl.R[q] == 2;
+    for (int q = 0; q < pl.nmid; ++q) bin_mid = bin_mid && pl.R[pl.nin + q] == 2;
     for (int t = tid; t < pl.Lin; t += T) {
         double w;
-        sm.tab_f[t] = gray_entry(pl, 0, pl.nin, pl.Pin, t, &w, t == pl.Lin - 1 ? sm.plan.vend : nullptr);
+        sm.tab_f[t] = gray_entry(pl, 0, pl.nin, pl.Pin, t, &w, t == pl.Lin - 1 ? sm.plan.vend : nullptr, bin_in);
         sm.tab_w[t] = w;
         sm.tab_w32[t] = (float)w;
     }
     for (int t = tid; t < pl.Lmid; t += T) {
         double w;
-        sm.tab_fm[t] = gray_entry(pl, pl.nin, pl.nmid, pl.Pmid, t, &w, nullptr);
+        sm.tab_fm[t] = gray_entry(pl, pl.nin, pl.nmid, pl.Pmid, t, &w, nullptr, bin_mid);
         sm.tab_wm[t] = w;
     }
 }
@@ -653,8 +691,9 @@ static __device__ __forceinline__ uint64_t lane_digits(const Plan& pl, int64_t h
     int64_t rem = hl;
     for (int i = 0; i < pl.nhi; ++i) {
         const int R = pl.R[hi0 + i];
-        const int v = (int)(rem % R);
-        rem /= R;
+        int v;
+        if (R == 2) { v = (int)(rem & 1); rem >>= 1; }      // the common radix without a 64-bit division
+        else { v = (int)(rem % R); rem /= R; }
         if (i < 12) packed |= (uint64_t)v << (5 * i);
         wh *= signed_binom(pl.M[hi0 + i], v);
     }
@@ -864,17 +903,36 @@ __device__ __forceinline__ void cofactor_step(Smem& sm, const double2* A, int64_
 static __device__ void draw_step(Smem& sm, double* __restrict__ wgt, const double2* __restrict__ A, int64_t rs, int64_t cs,
                                  int m, int k, double u, double* __restrict__ marg_row, bool update_groups) {
     const int tid = threadIdx.x, T = blockDim.x, lid = tid & 31, wid = tid >> 5, nw = T >> 5;
-    for (int rho = tid; rho < m; rho += T) {
-        double xr = 0.0, xi = 0.0;
+    // DR modes per thread at a time, so that DR independent loads of A (from L2) are in flight per
+    // column instead of one; the sum over columns keeps its order (same bits as one mode at a time)
+    constexpr int DR = 4;
+    for (int rho0 = tid; rho0 < m; rho0 += T * DR) {
+        double xr[DR], xi[DR];
+#pragma unroll
+        for (int r = 0; r < DR; ++r) { xr[r] = 0.0; xi[r] = 0.0; }
+#pragma unroll 2
         for (int c = 0; c < k; ++c) {
-            const double2 a = A[(int64_t)rho * rs + (int64_t)sm.cols[c] * cs];
+            const int64_t co = (int64_t)sm.cols[c] * cs;
             const double2 p = sm.P[c];
-            xr = fma(a.x, p.x, xr);
-            xr = fma(-a.y, p.y, xr);
-            xi = fma(a.x, p.y, xi);
-            xi = fma(a.y, p.x, xi);
+            double2 a[DR];
+#pragma unroll
+            for (int r = 0; r < DR; ++r) {
+                const int rho = rho0 + r * T;
+                a[r] = rho < m ? A[(int64_t)rho * rs + co] : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int r = 0; r < DR; ++r) {
+                xr[r] = fma(a[r].x, p.x, xr[r]);
+                xr[r] = fma(-a[r].y, p.y, xr[r]);
+                xi[r] = fma(a[r].x, p.y, xi[r]);
+                xi[r] = fma(a[r].y, p.x, xi[r]);
+            }
         }
-        wgt[rho] = xr * xr + xi * xi;
+#pragma unroll
+        for (int r = 0; r < DR; ++r) {
+            const int rho = rho0 + r * T;
+            if (rho < m) wgt[rho] = xr[r] * xr[r] + xi[r] * xi[r];
+        }
     }
     __syncthreads();
     const int C = (m + T - 1) / T;
@@ -963,7 +1021,7 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
         return;
     }
     if (kf > 1) {
-        if (tid == 0) for (int i = 0; i < kf - 1; ++i) add_to_groups(sm, sm.rows[i]);
+        if (tid < 32) build_groups_warp(sm, kf - 1);
         __syncthreads();
     }
     const double2* A = p.acol + off;      // (rho, j) at A[j * m + rho]
@@ -1078,7 +1136,7 @@ static __device__ bool load_state(const ChainParams& p, Smem& sm, int64_t s, int
         if (tid == 0) record_error(p.status, p.detail, s);
         return false;
     }
-    if (tid == 0) for (int i = 0; i < k - 1; ++i) add_to_groups(sm, sm.rows[i]);
+    if (tid < 32) build_groups_warp(sm, k - 1);
     __syncthreads();
     return true;
 }
@@ -1094,7 +1152,7 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_partial_kernel(SplitPa
         const int i = (int)(item % sp.nch);
         int m;
         int64_t off;
-        const bool live = load_state(p, sm, s, k, m, off) && (sp.pass == 0 || sp.flag[s] != 0);
+        const bool live = (sp.pass == 0 || sp.flag[s] != 0) && load_state(p, sm, s, k, m, off);
         if (live) {
             if (tid == 0) { sm.lane0 = (int64_t)i * (blockDim.x / TPL); sm.lane_mult = sp.nch; }
             __syncthreads();
@@ -1117,10 +1175,11 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_draw_kernel(SplitParam
     for (int64_t s = blockIdx.x; s < p.S; s += gridDim.x) {
         int m;
         int64_t off;
-        if (!load_state(p, sm, s, k, m, off) || (sp.pass == 1 && sp.flag[s] == 0)) { __syncthreads(); continue; }
+        if ((sp.pass == 1 && sp.flag[s] == 0) || !load_state(p, sm, s, k, m, off)) { __syncthreads(); continue; }
         if (tid < k) {
             double xr = 0.0, xi = 0.0;
-            for (int i = 0; i < sp.nch; ++i) {
+#pragma unroll 8
+            for (int i = 0; i < sp.nch; ++i) {                 // fixed order; unrolled: loads in flight
                 const double2 v = sp.partial[(s * sp.nch + i) * MAXN + tid];
                 xr += v.x;
                 xi += v.y;
@@ -1182,7 +1241,7 @@ __global__ void __launch_bounds__(256) cofactor_kernel(const double2* __restrict
             __syncthreads();
             continue;
         }
-        if (tid == 0) for (int i = 0; i < K - 1; ++i) add_to_groups(sm, sm.rows[i]);
+        if (tid < 32) build_groups_warp(sm, K - 1);
         __syncthreads();
         if (K == 1) {
             if (tid == 0) sm.P[0] = make_double2(1.0, 0.0);

@@ -46,15 +46,18 @@ static __device__ void prepare_warp(WarpSmem& sm, const double2* __restrict__ A,
         sm.B[kd][j] = b;
         if (mixed) sm.B32[kd][j] = make_float2((float)(2.0 * b.x), (float)(2.0 * b.y));
     }
+    bool bin_in = true, bin_mid = true;             // schedules of radix-2 digits only (distinct rows)
+    for (int q = 0; q < pl.nin; ++q) bin_in = bin_in && pl.R[q] == 2;
+    for (int q = 0; q < pl.nmid; ++q) bin_mid = bin_mid && pl.R[pl.nin + q] == 2;
     for (int t = lane; t < pl.Lin; t += 32) {
         double w;
-        sm.tab_f[t] = gray_entry(pl, 0, pl.nin, pl.Pin, t, &w, t == pl.Lin - 1 ? sm.plan.vend : nullptr);
+        sm.tab_f[t] = gray_entry(pl, 0, pl.nin, pl.Pin, t, &w, t == pl.Lin - 1 ? sm.plan.vend : nullptr, bin_in);
         sm.tab_w[t] = w;
         sm.tab_w32[t] = (float)w;
     }
     for (int t = lane; t < pl.Lmid; t += 32) {
         double w;
-        sm.tab_fm[t] = gray_entry(pl, pl.nin, pl.nmid, pl.Pmid, t, &w, nullptr);
+        sm.tab_fm[t] = gray_entry(pl, pl.nin, pl.nmid, pl.Pmid, t, &w, nullptr, bin_mid);
         sm.tab_wm[t] = w;
     }
 }
@@ -199,7 +202,8 @@ static __device__ double draw_warp(WarpSmem& sm, const double2* __restrict__ A, 
             double w = 0.0;
             if (rho < m) {
                 double xr = 0.0, xi = 0.0;
-                for (int c = 0; c < k; ++c) {
+#pragma unroll 4
+                for (int c = 0; c < k; ++c) {                  // unrolled: several loads in flight
                     const double2 a = A[(int64_t)rho + (int64_t)sm.cols[c] * m];
                     const double2 p = sm.P[c];
                     xr = fma(a.x, p.x, xr);
@@ -267,10 +271,8 @@ __device__ void chain_warp(const ChainParams& p, WarpSmem& sm, int64_t s) {
         __syncwarp();
         return;
     }
-    if (lane == 0) {
-        sm.ngrp = 0; sm.lane0 = 0; sm.lane_mult = 1;
-        for (int i = 0; i < kf - 1; ++i) add_to_groups(sm, sm.rows[i]);
-    }
+    build_groups_warp(sm, kf - 1);
+    if (lane == 0) { sm.lane0 = 0; sm.lane_mult = 1; }
     __syncwarp();
     const double2* A = p.acol + off;
     const int kend = (p.k_stop > 0 && p.k_stop < nk) ? p.k_stop : nk;

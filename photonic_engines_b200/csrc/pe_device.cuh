@@ -49,6 +49,9 @@ static __device__ __forceinline__ double chain_uniform(uint64_t seed, int64_t of
 // ------------------------------------------------------------------------------------------ maths
 // (-1)^v C(M, v), exact: the integer product is formed in int64 (M <= 32) before conversion.
 static __device__ __forceinline__ double signed_binom(int M, int v) {
+    if (v == 0) return 1.0;                          // the usual multiplicities without 64-bit divisions
+    if (v == 1) return -(double)M;
+    if (v == 2) return (double)(M * (M - 1) / 2);
     int64_t c = 1;
     for (int i = 0; i < v; ++i) c = c * (M - i) / (i + 1);
     return (v & 1) ? -(double)c : (double)c;
