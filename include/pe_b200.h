@@ -49,12 +49,14 @@ extern "C" {
 #define PE_PRECISION_F64 0     /* complex FP64 throughout: the drop-in form */
 #define PE_PRECISION_MIXED 1   /* FP32 Gray blocks, FP64 cross-block sum, FP64 marginal and CDF */
 
-#define PE_MAX_PHOTONS 32      /* photons per stream (cofactor tiers up to 32 columns) */
+#define PE_MAX_PHOTONS 64      /* photons per stream (cofactor tiers up to 64 columns) */
+#define PE_MIXED_MAX_PHOTONS 32 /* the mixed form (FP32 Gray blocks) up to 32; FP64 beyond */
 
 /* Library version (major * 10000 + minor * 100 + patch). */
 int pe_version(void);
 
-/* Largest supported number of output modes for the given block size (shared-memory bound). */
+/* Largest supported number of output modes for chains of up to 32 photons (shared-memory bound; the
+ * wider tables of 33-64 photons leave fewer: pe_fock_chain answers PE_ERR_SIZE beyond them). */
 int pe_max_modes(int block_threads);
 
 /* Bytes of device workspace that pe_fock_chain needs (16-byte aligned pointer). */

@@ -18,7 +18,9 @@ CANDIDATES = {8: [(1, 128), (1, 256), (2, 128), (2, 256)],
               20: [(1, 128), (2, 128), (2, 256), (4, 128), (4, 256)],
               24: [(2, 64), (2, 128), (4, 128), (4, 256)],
               28: [(2, 64), (2, 128), (4, 128), (4, 256)],
-              32: [(2, 64), (2, 128), (4, 128), (4, 256)]}
+              32: [(2, 64), (2, 128), (4, 128), (4, 256)],
+              40: [(4, 64), (4, 128)], 48: [(4, 64), (4, 128)], 56: [(4, 64), (4, 128)],
+              64: [(4, 64), (4, 128)]}
 
 
 def _cache_path() -> str:
@@ -50,12 +52,12 @@ def tier(n: int) -> int:
     for k in sorted(CANDIDATES):
         if n <= k:
             return k
-    raise ValueError(f"at most 32 photons (got {n})")
+    raise ValueError(f"at most 64 photons (got {n})")
 
 
 # bumped whenever the compiled launch shapes change, so that a cached choice the library no longer accepts
 # is never replayed
-SHAPES_VERSION = 2
+SHAPES_VERSION = 3
 
 
 def key(device, precision: str, workload: str) -> str:

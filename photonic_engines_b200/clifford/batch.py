@@ -70,8 +70,7 @@ class BatchedSampler:
         self.m = [int(U.shape[0]) for U, _ in circuits]
         self.n = [len(modes) for _, modes in circuits]
         self.m_max, self.n_stride = max(self.m), max(max(self.n), 1)
-        if self.n_stride > N.PE_MAX_PHOTONS:
-            raise ValueError(f"at most {N.PE_MAX_PHOTONS} photons per circuit")
+        N.check_photons(self.n_stride, precision, "photons per circuit")
         self.S = sum(shots_l)
         self.acol, self.inst_off, self.inst_m, self.inst_n = pack_ragged(circuits)
         self.acol = torch.view_as_real(self.acol).contiguous()

@@ -72,10 +72,10 @@ DEFAULT_BLOCK = 128          # the library's CTA size when the caller passes 0 (
 
 def default_tpl(n: int, precision: str) -> int:
     """Threads per Gray lane the library picks when the caller passes 0 (fock_api.cu default_tpl)."""
-    kpm = next((k for k in (8, 16, 20, 24, 28, 32) if n <= k), 32)
+    kpm = next((k for k in (8, 16, 20, 24, 28, 32, 40, 48, 56, 64) if n <= k), 64)
     if kpm <= 8 or (precision == "f64" and kpm == 20):
         return 1
-    return 2
+    return 2 if kpm <= 32 else 4
 
 
 NCH_MAX = 64                 # CTAs per stream at most
@@ -159,8 +159,7 @@ def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst
     dp = _i64(dp, dev)
     cols = _i64(cols, dev)
     S, n_stride = cols.shape
-    if n_stride > N.PE_MAX_PHOTONS:
-        raise ValueError(f"at most {N.PE_MAX_PHOTONS} photons per stream (got {n_stride})")
+    N.check_photons(n_stride, precision)
     if m_max is None:
         m_max = int(inst_m.max().item())
     occ_stride = occ_stride or m_max
@@ -229,8 +228,7 @@ def chain_adaptive(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Ten
     dp = _i64(dp, dev)
     cols = _i64(cols, dev)
     S, n = cols.shape
-    if n > N.PE_MAX_PHOTONS:
-        raise ValueError(f"at most {N.PE_MAX_PHOTONS} photons per stream (got {n})")
+    N.check_photons(n, precision)
     if m_max is None:
         m_max = int(inst_m.max().item())
     u_t = None if uniforms is None else torch.as_tensor(uniforms, dtype=torch.float64, device=dev).contiguous()
@@ -275,6 +273,7 @@ def laplace_cofactors_rows(A: torch.Tensor, rows: torch.Tensor, precision: str =
     (repeats allowed).  Same contract as the reference's laplace_cofactors_rows."""
     N.require_cuda(A, "A")
     S, m, K = A.shape
+    N.check_photons(K, precision, "columns")
     dev = A.device
     A2 = torch.view_as_real(A.to(torch.complex128).contiguous())
     rows = torch.as_tensor(rows, dtype=torch.int64, device=dev).reshape(S, K - 1).contiguous()

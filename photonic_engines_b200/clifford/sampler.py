@@ -148,8 +148,7 @@ def fock_sample(U, in_modes, shots, generator=None, algo="auto", multi_min_k1=10
     Bn, m, _ = U.shape
     n = len(in_modes)
     dev = U.device
-    if n > N.PE_MAX_PHOTONS:
-        raise ValueError(f"at most {N.PE_MAX_PHOTONS} photons (got {n})")
+    N.check_photons(n, precision, "photons")
     if any(not 0 <= int(j) < m for j in in_modes):
         raise ValueError(f"in_modes {list(in_modes)}: input modes of the circuit")
     lossless = loss is None or float(loss) >= 1.0

@@ -12,8 +12,8 @@
 
 namespace pe {
 
-constexpr int N_KPM = 6;
-constexpr int KPM_LADDER[N_KPM] = {8, 16, 20, 24, 28, 32};
+constexpr int N_KPM = 10;
+constexpr int KPM_LADDER[N_KPM] = {8, 16, 20, 24, 28, 32, 40, 48, 56, 64};
 static int kpm_for(int n) {
     for (int i = 0; i < N_KPM; ++i) if (n <= KPM_LADDER[i]) return KPM_LADDER[i];
     return -1;
@@ -69,7 +69,7 @@ void* find_cofactor_kernel(int mixed, int tpl, int kpm) {
 static int default_tpl(int kpm, int precision) {
     if (kpm <= 8) return 1;
     if (precision == PE_PRECISION_F64 && kpm == 20) return 1;
-    return 2;
+    return kpm <= NARROW ? 2 : 4;
 }
 
 static thread_local cudaError_t g_last_cuda_error = cudaSuccess;
@@ -195,7 +195,7 @@ extern "C" int pe_max_modes(int block_threads) {
     (void)block_threads;
     const int cap = max_smem_optin();
     if (cap <= 0) return 0;
-    return (int)((cap - (int)smem_fixed_bytes()) / (int)sizeof(double));
+    return (int)((cap - (int)smem_fixed_bytes_for(NARROW)) / (int)sizeof(double));
 }
 
 extern "C" size_t pe_chain_workspace_bytes(int64_t S) {
@@ -267,6 +267,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     if (workspace_bytes < need || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
     const int kpm = kpm_for(n_stride);
     if (kpm < 0) return PE_ERR_SIZE;
+    if (kpm > NARROW && precision != PE_PRECISION_F64) return PE_ERR_SIZE;   // mixed form: up to 32 columns
     if (warp_mode && (kpm > WMAXN || split)) return PE_ERR_SIZE;
     if (tpl == 0) {
         tpl = warp_mode ? (kpm <= 8 ? 1 : 2) : default_tpl(kpm, precision);
@@ -280,8 +281,8 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     // default CTA: 128 threads (as many warps per SM as 256-thread CTAs, twice the CTAs to overlap the
     // per-step serial phases of one stream with the sweeps of others)
     const int block = warp_mode ? 32 * WARPS : (block_threads ? block_threads : (bmax < 128 ? bmax : 128));
-    if (block < 32 || block > 256 || block > bmax || (block & 31)) return PE_ERR_ARG;
-    const size_t smem = warp_mode ? warp_smem_bytes() : smem_fixed_bytes() + (size_t)m_max * sizeof(double);
+    if (block < 32 || block > 256 || block > bmax || (block & 31) || block < n_stride) return PE_ERR_ARG;
+    const size_t smem = warp_mode ? warp_smem_bytes() : smem_fixed_bytes_for(kpm) + (size_t)m_max * sizeof(double);
     const int cap = max_smem_optin();
     if (cap <= 0) return PE_ERR_CUDA;
     if (smem > (size_t)cap) return PE_ERR_SIZE;
@@ -324,7 +325,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     for (int q = 0; q < npass; ++q) {
         if (!fpart[q] || !fdraw[q]) return PE_ERR_SIZE;
         int per_part = 0, per_draw = 0;
-        if ((rc = launch_prepare(fpart[q], block, smem_fixed_bytes(), &per_part)) != PE_OK) return rc;
+        if ((rc = launch_prepare(fpart[q], block, smem_fixed_bytes_for(kpm), &per_part)) != PE_OK) return rc;
         if ((rc = launch_prepare(fdraw[q], block, smem, &per_draw)) != PE_OK) return rc;
         gpart[q] = items < (int64_t)sms * per_part ? items : (int64_t)sms * per_part;
         gdraw[q] = S < (int64_t)sms * per_draw ? S : (int64_t)sms * per_draw;
@@ -339,7 +340,8 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
         sp.k = k;
         for (int q = 0; q < npass; ++q) {
             sp.pass = q;
-            PE_CUDA_TRY(cudaLaunchKernel(fpart[q], dim3((unsigned)gpart[q]), dim3(block), sargs, smem_fixed_bytes(), st));
+            PE_CUDA_TRY(cudaLaunchKernel(fpart[q], dim3((unsigned)gpart[q]), dim3(block), sargs, smem_fixed_bytes_for(kpm),
+                                         st));
             PE_CUDA_TRY(cudaLaunchKernel(fdraw[q], dim3((unsigned)gdraw[q]), dim3(block), sargs, smem, st));
         }
     }
@@ -457,18 +459,19 @@ extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t
     if (workspace_bytes < WS_BYTES || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
     const int kpm = kpm_for(K);
     if (kpm < 0) return PE_ERR_SIZE;
-    if (tpl == 0) tpl = kpm <= 8 ? 1 : 2;
+    if (kpm > NARROW && precision != PE_PRECISION_F64) return PE_ERR_SIZE;
+    if (tpl == 0) tpl = kpm <= 8 ? 1 : (kpm <= NARROW ? 2 : 4);
     if (tpl_index(tpl) < 0) return PE_ERR_ARG;
     void* fn = find_cofactor_kernel(precision, tpl, kpm);
     if (!fn) return PE_ERR_SIZE;
     const int bmax = max_block(fn);
     if (bmax < 32) return PE_ERR_CUDA;
     const int block = block_threads ? block_threads : (bmax < 256 ? bmax : 256);
-    if (block < 32 || block > 256 || block > bmax || (block & 31)) return PE_ERR_ARG;
+    if (block < 32 || block > 256 || block > bmax || (block & 31) || block < K) return PE_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     PE_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, WS_BYTES, st));
     if (S == 0) return PE_OK;
-    const size_t smem = smem_fixed_bytes();
+    const size_t smem = smem_fixed_bytes_for(kpm);
     int per_sm = 0;
     int rc = launch_prepare(fn, block, smem, &per_sm);
     if (rc != PE_OK) return rc;
@@ -490,6 +493,7 @@ extern "C" int pe_split_slots(int precision, int n_stride, int block_threads, in
     if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
     const int kpm = kpm_for(n_stride);
     if (n_stride < 1 || kpm < 0) return PE_ERR_SIZE;
+    if (kpm > NARROW && precision != PE_PRECISION_F64) return PE_ERR_SIZE;
     if (tpl == 0) {
         tpl = default_tpl(kpm, precision);
         if (!find_chain_kernel(precision, tpl, kpm)) tpl = find_chain_kernel(precision, 2, kpm) ? 2 : 4;
@@ -502,7 +506,7 @@ extern "C" int pe_split_slots(int precision, int n_stride, int block_threads, in
     const int block = block_threads ? block_threads : (bmax < 128 ? bmax : 128);
     if (block < 32 || block > 256 || block > bmax || (block & 31)) return PE_ERR_ARG;
     int per_sm = 0, dev = 0, sms = 0;
-    const int rc = launch_prepare(fn, block, smem_fixed_bytes(), &per_sm);
+    const int rc = launch_prepare(fn, block, smem_fixed_bytes_for(kpm), &per_sm);
     if (rc != PE_OK) return rc;
     PE_CUDA_TRY(cudaGetDevice(&dev));
     PE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

@@ -110,6 +110,14 @@ __device__ __forceinline__ void add_to_groups(SM& sm, int row) {
 template <class SM>
 __device__ __forceinline__ void build_groups_warp(SM& sm, int count) {
     const int lane = threadIdx.x & 31;
+    if (count > 32) {                                          // chains beyond 33 photons: serial
+        if (lane == 0) {
+            sm.ngrp = 0;
+            for (int i = 0; i < count; ++i) add_to_groups(sm, sm.rows[i]);
+        }
+        __syncwarp();
+        return;
+    }
     const bool has = lane < count;
     const int row = has ? sm.rows[lane] : -1 - lane;          // absent lanes: distinct non-rows
     const unsigned same = __match_any_sync(0xffffffffu, row);
@@ -132,25 +140,43 @@ __device__ __forceinline__ void build_groups_warp(SM& sm, int count) {
 // middle block; what does not fit the schedules joins the lanes.
 template <class SM>
 __device__ void plan_step(SM& sm, int K1, int K, int lanes, int lin_max, int mid_max) {
-    Plan& pl = sm.plan;
+    auto& pl = sm.plan;
+    constexpr int GL = (SM::NKMAX + 31) / 32;          // groups per lane: group lane + 32 q, q < GL
     const int lane = threadIdx.x & 31;
     const int D = sm.ngrp;
-    const bool has = lane < D;
-    const int M = has ? sm.gmul[lane] : 0;
-    const unsigned oddmask = __ballot_sync(0xffffffffu, has && (M & 1));
-    const int halved = oddmask ? 31 - __clz(oddmask) : -1;
-    const int R = has ? (lane == halved ? (M + 1) / 2 : M + 1) : 1;
-    const bool active = R >= 2;
-    int rank = 0;
-    for (int j = 0; j < 32; ++j) {
-        const int Rj = __shfl_sync(0xffffffffu, R, j);
-        if (Rj >= 2 && active && (Rj < R || (Rj == R && j < lane))) ++rank;
+    int halved = -1;                                   // the last group of odd multiplicity
+#pragma unroll
+    for (int q = 0; q < GL; ++q) {
+        const int g = lane + 32 * q;
+        const unsigned oddmask = __ballot_sync(0xffffffffu, g < D && (sm.gmul[g < D ? g : 0] & 1));
+        if (oddmask) halved = 32 * q + 31 - __clz(oddmask);
     }
-    if (active) { pl.sortR[rank] = R; pl.sortG[rank] = lane; }
+    int R[GL];
+    bool active[GL];
+#pragma unroll
+    for (int q = 0; q < GL; ++q) {
+        const int g = lane + 32 * q;
+        const int M = g < D ? sm.gmul[g] : 0;
+        R[q] = g < D ? (g == halved ? (M + 1) / 2 : M + 1) : 1;
+        active[q] = R[q] >= 2;
+    }
+    int na = 0;
+#pragma unroll
+    for (int q = 0; q < GL; ++q) {
+        int rank = 0;                                  // among active groups, by (radix, group)
+#pragma unroll
+        for (int q2 = 0; q2 < GL; ++q2) {
+            for (int j = 0; j < 32; ++j) {
+                const int Rj = __shfl_sync(0xffffffffu, R[q2], j);
+                const int gj = j + 32 * q2, g = lane + 32 * q;
+                if (Rj >= 2 && active[q] && (Rj < R[q] || (Rj == R[q] && gj < g))) ++rank;
+            }
+        }
+        if (active[q]) { pl.sortR[rank] = R[q]; pl.sortG[rank] = lane + 32 * q; }
+        na += __popc(__ballot_sync(0xffffffffu, active[q]));
+    }
     __syncwarp();
-    const unsigned actmask = __ballot_sync(0xffffffffu, active);
     if (lane == 0) {
-        const int na = __popc(actmask);
         int64_t N = 1;
         for (int i = 0; i < na; ++i) N *= pl.sortR[i];
         // lanes: the prefix of the ranked digits that best fills the CTA's lanes
@@ -222,7 +248,8 @@ __device__ void plan_step(SM& sm, int K1, int K, int lanes, int lin_max, int mid
 // One index of a reflected mixed-radix Gray schedule over `nd` digits starting at kernel digit
 // `d0` with radices R and prefix products Pp: its weight prod (-1)^v C(M, v) and the transition
 // into it (the digit the odometer moved, and the sign of the column-sum update -2 dir b).
-static __device__ __forceinline__ unsigned char gray_entry(const Plan& pl, int d0, int nd, const int* Pp, int t,
+template <class PL>
+static __device__ __forceinline__ unsigned char gray_entry(const PL& pl, int d0, int nd, const int* Pp, int t,
                                                           double* w_out, unsigned char* vend, bool binary) {
     if (binary) {                                   // every radix 2: the digits are the bits of t
         const int qstar = t > 0 ? __ffs(t) - 1 : -1;
@@ -266,26 +293,30 @@ static __device__ __forceinline__ unsigned char gray_entry(const Plan& pl, int d
 // paired FP32 sweeps, kh columns per thread): row kd of B32 is written as float4 slots
 // q = h * kh/2 + c holding (re b_j1, re b_j2, im b_j1, im b_j2) of 2b, j1 = h * kh + c, j2 = j1 + kh/2 —
 // the two columns whose product chains one paired instruction advances together.
-static __device__ void prepare_step(Smem& sm, const double2* __restrict__ A, int64_t rs, int64_t cs, bool mixed,
+template <class SM>
+static __device__ void prepare_step(SM& sm, const double2* __restrict__ A, int64_t rs, int64_t cs, bool mixed,
                                     int kh = 0) {
-    const Plan& pl = sm.plan;
+    constexpr int NK = SM::NKMAX;
+    constexpr bool narrow = SM::NK32 == NK;           // the wide layout has no FP32 copy (FP64 only)
+    const auto& pl = sm.plan;
     const int tid = threadIdx.x, T = blockDim.x;
-    for (int idx = tid; idx < pl.D * MAXN; idx += T) {
-        const int kd = idx / MAXN, j = idx % MAXN;
+    for (int idx = tid; idx < pl.D * NK; idx += T) {
+        const int kd = idx / NK, j = idx % NK;
         double2 b = make_double2(0.0, 0.0);
         if (j < pl.K) b = A[(int64_t)pl.drow[kd] * rs + (int64_t)sm.cols[j] * cs];
         sm.B[kd][j] = b;
-        if (mixed && kh == 0) sm.B32[kd][j] = make_float2((float)(2.0 * b.x), (float)(2.0 * b.y));
+        if constexpr (narrow)
+            if (mixed && kh == 0) sm.B32[kd][j] = make_float2((float)(2.0 * b.x), (float)(2.0 * b.y));
     }
-    if (mixed && kh > 0) {
+    if (narrow && mixed && kh > 0) {
         __syncthreads();
         const int ka = kh / 2;
-        for (int idx = tid; idx < pl.D * (MAXN / 2); idx += T) {
-            const int kd = idx / (MAXN / 2), q = idx % (MAXN / 2);
+        for (int idx = tid; idx < pl.D * (NK / 2); idx += T) {
+            const int kd = idx / (NK / 2), q = idx % (NK / 2);
             const int j1 = (q / ka) * kh + q % ka, j2 = j1 + ka;
             const double2 b1 = j1 < pl.K ? sm.B[kd][j1] : make_double2(0.0, 0.0);
             const double2 b2 = j2 < pl.K ? sm.B[kd][j2] : make_double2(0.0, 0.0);
-            reinterpret_cast<float4*>(&sm.B32[kd][0])[q] =
+            reinterpret_cast<float4*>(&sm.B32[kd < SM::NK32 ? kd : 0][0])[q] =
                 make_float4((float)(2.0 * b1.x), (float)(2.0 * b2.x), (float)(2.0 * b1.y), (float)(2.0 * b2.y));
         }
     }
@@ -306,7 +337,8 @@ static __device__ void prepare_step(Smem& sm, const double2* __restrict__ A, int
 }
 
 // Middle digit values at middle index pm (the reflected Gray code decoded directly).
-static __device__ __forceinline__ int middle_digit(const Plan& pl, int pm, int q) {
+template <class PL>
+static __device__ __forceinline__ int middle_digit(const PL& pl, int pm, int q) {
     int par = 0, v = 0;
     for (int i = pl.nmid - 1; i >= q; --i) {
         const int R = pl.R[pl.nin + i];
@@ -658,8 +690,8 @@ __device__ __forceinline__ void inner_block_pair(float2 (&sr)[KH / 2], float2 (&
 }
 
 // Deterministic reduction of the per-thread accumulators over the lanes of the CTA -> sm.P.
-template <int KH, int TPL>
-__device__ __forceinline__ void reduce_to_P(double (&ar)[KH], double (&ai)[KH], Smem& sm, int c0) {
+template <int KH, int TPL, class SM>
+__device__ __forceinline__ void reduce_to_P(double (&ar)[KH], double (&ai)[KH], SM& sm, int c0) {
     const int tid = threadIdx.x, lid = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
 #pragma unroll
     for (int j = 0; j < KH; ++j) {
@@ -682,9 +714,16 @@ __device__ __forceinline__ void reduce_to_P(double (&ar)[KH], double (&ai)[KH], 
     __syncthreads();
 }
 
-// High-digit values of Gray lane hl (plain mixed radix over the high digits), packed 5 bits per digit
-// (radices <= 32), and the lane's weight prod (-1)^v C(M, v) over them.
-static __device__ __forceinline__ uint64_t lane_digits(const Plan& pl, int64_t hl, double* wh_out) {
+// High-digit values of Gray lane hl (plain mixed radix over the high digits), packed HBITS bits per
+// digit for the first HDIG digits (5 x 12 when radices are <= 32, 6 x 10 for the wide tiers), and the
+// lane's weight prod (-1)^v C(M, v) over them.
+template <class PL>
+struct HighPack {
+    static constexpr int HBITS = PL::NKMAX <= NARROW ? 5 : 6;
+    static constexpr int HDIG = 60 / HBITS;
+};
+template <class PL>
+static __device__ __forceinline__ uint64_t lane_digits(const PL& pl, int64_t hl, double* wh_out) {
     const int hi0 = pl.nin + pl.nmid;
     uint64_t packed = 0;
     double wh = 1.0;
@@ -694,7 +733,7 @@ static __device__ __forceinline__ uint64_t lane_digits(const Plan& pl, int64_t h
         int v;
         if (R == 2) { v = (int)(rem & 1); rem >>= 1; }      // the common radix without a 64-bit division
         else { v = (int)(rem % R); rem /= R; }
-        if (i < 12) packed |= (uint64_t)v << (5 * i);
+        if (i < HighPack<PL>::HDIG) packed |= (uint64_t)v << (HighPack<PL>::HBITS * i);
         wh *= signed_binom(pl.M[hi0 + i], v);
     }
     *wh_out = wh;
@@ -707,7 +746,8 @@ static __device__ __forceinline__ uint64_t lane_digits(const Plan& pl, int64_t h
 template <int KH, class SM>
 __device__ __forceinline__ void lane_sums(const SM& sm, int c0, bool inner_end, int pm, int64_t hl, uint64_t hpack,
                                           double (&xr)[KH], double (&xi)[KH]) {
-    const Plan& pl = sm.plan;
+    const auto& pl = sm.plan;
+    using HP = HighPack<decltype(sm.plan)>;
 #pragma unroll
     for (int j = 0; j < KH; ++j) { xr[j] = 0.0; xi[j] = 0.0; }
     const int nin = pl.nin, nmid = pl.nmid, hi0 = nin + nmid, nhi = pl.nhi;
@@ -729,8 +769,8 @@ __device__ __forceinline__ void lane_sums(const SM& sm, int c0, bool inner_end, 
     int64_t rem = hl;
     for (int i = 0; i < nhi; ++i) {
         int v;
-        if (i < 12) {
-            v = (int)((hpack >> (5 * i)) & 31u);
+        if (i < HP::HDIG) {
+            v = (int)((hpack >> (HP::HBITS * i)) & ((1u << HP::HBITS) - 1u));
         } else {
             int64_t r2 = hl;
             for (int q = 0; q < i; ++q) r2 /= pl.R[hi0 + q];
@@ -743,10 +783,10 @@ __device__ __forceinline__ void lane_sums(const SM& sm, int c0, bool inner_end, 
 }
 
 // FP64 sweep of tier KP (columns padded to KP: padded column sums hold 1, their B rows are zero).
-template <int KP, int TPL>
-__device__ void sweep_f64(Smem& sm) {
+template <int KP, int TPL, class SM>
+__device__ void sweep_f64(SM& sm) {
     constexpr int KH = KP / TPL;
-    const Plan& pl = sm.plan;
+    const auto& pl = sm.plan;
     const int tid = threadIdx.x;
     const int lanes = blockDim.x / TPL, lane = tid / TPL, h = tid % TPL, c0 = h * KH;
     const int wl0 = (tid & ~31) / TPL;                     // first lane of this warp
@@ -784,10 +824,10 @@ __device__ void sweep_f64(Smem& sm) {
 
 // Mixed sweep: every inner block starts from column sums formed in FP64 from the digit values
 // (no drift carried across blocks), runs in complex FP32, and is folded into FP64 accumulators.
-template <int KP, int TPL>
-__device__ void sweep_mixed(Smem& sm) {
+template <int KP, int TPL, class SM>
+__device__ void sweep_mixed(SM& sm) {
     constexpr int KH = KP / TPL;
-    const Plan& pl = sm.plan;
+    const auto& pl = sm.plan;
     const int tid = threadIdx.x;
     const int lanes = blockDim.x / TPL, lane = tid / TPL, h = tid % TPL, c0 = h * KH;
     const int wl0 = (tid & ~31) / TPL;
@@ -858,8 +898,8 @@ __device__ void sweep_mixed(Smem& sm) {
         if (K <= KPv) { CALL; return; }                      \
     }
 
-template <int TPL, int KPM>
-__device__ void dispatch_f64(Smem& sm, int K) {
+template <int TPL, int KPM, class SM>
+__device__ void dispatch_f64(SM& sm, int K) {
     PE_TIER(4, (sweep_f64<4, TPL>(sm)))
     PE_TIER(8, (sweep_f64<8, TPL>(sm)))
     PE_TIER(12, (sweep_f64<12, TPL>(sm)))
@@ -868,10 +908,18 @@ __device__ void dispatch_f64(Smem& sm, int K) {
     PE_TIER(24, (sweep_f64<24, TPL>(sm)))
     PE_TIER(28, (sweep_f64<28, TPL>(sm)))
     PE_TIER(32, (sweep_f64<32, TPL>(sm)))
+    PE_TIER(36, (sweep_f64<36, TPL>(sm)))
+    PE_TIER(40, (sweep_f64<40, TPL>(sm)))
+    PE_TIER(44, (sweep_f64<44, TPL>(sm)))
+    PE_TIER(48, (sweep_f64<48, TPL>(sm)))
+    PE_TIER(52, (sweep_f64<52, TPL>(sm)))
+    PE_TIER(56, (sweep_f64<56, TPL>(sm)))
+    PE_TIER(60, (sweep_f64<60, TPL>(sm)))
+    PE_TIER(64, (sweep_f64<64, TPL>(sm)))
 }
 
-template <int TPL, int KPM>
-__device__ void dispatch_mixed(Smem& sm, int K) {
+template <int TPL, int KPM, class SM>
+__device__ void dispatch_mixed(SM& sm, int K) {
     PE_TIER(4, (sweep_mixed<4, TPL>(sm)))
     PE_TIER(8, (sweep_mixed<8, TPL>(sm)))
     PE_TIER(12, (sweep_mixed<12, TPL>(sm)))
@@ -883,8 +931,8 @@ __device__ void dispatch_mixed(Smem& sm, int K) {
 }
 
 // One cofactor step of the stream held in shared memory (K1 >= 1): plan, prepare, sweep.
-template <int TPL, int KPM, bool MIXED>
-__device__ __forceinline__ void cofactor_step(Smem& sm, const double2* A, int64_t rs, int64_t cs, int K1, int K) {
+template <int TPL, int KPM, bool MIXED, class SM>
+__device__ __forceinline__ void cofactor_step(SM& sm, const double2* A, int64_t rs, int64_t cs, int K1, int K) {
     if (threadIdx.x < 32) plan_step(sm, K1, K, blockDim.x / TPL * sm.lane_mult, MIXED ? MIXED_LIN : LIN_MAX, MID_MAX);
     __syncthreads();
     // paired FP32 sweeps (mixed form, 1- and 2-thread lanes): columns per thread of the dispatched tier
@@ -900,7 +948,8 @@ __device__ __forceinline__ void cofactor_step(Smem& sm, const double2* A, int64_
 // in order), then idx = min(#{rho : cw_rho < u * tot}, m - 1) with tot = cw[m - 1]
 // (cofactors_triton.py:298-308).  Thread 0 records the pick and updates the groups; the gap
 // min |cw - u tot| / tot is left in sm.fmin[0].
-static __device__ void draw_step(Smem& sm, double* __restrict__ wgt, const double2* __restrict__ A, int64_t rs, int64_t cs,
+template <class SM>
+static __device__ void draw_step(SM& sm, double* __restrict__ wgt, const double2* __restrict__ A, int64_t rs, int64_t cs,
                                  int m, int k, double u, double* __restrict__ marg_row, bool update_groups) {
     const int tid = threadIdx.x, T = blockDim.x, lid = tid & 31, wid = tid >> 5, nw = T >> 5;
     // DR modes per thread at a time, so that DR independent loads of A (from L2) are in flight per
@@ -992,7 +1041,7 @@ static __device__ void draw_step(Smem& sm, double* __restrict__ wgt, const doubl
 
 // ---------------------------------------------------------------------------------------- chain
 template <int TPL, int KPM, bool MIXED>
-__device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s) {
+__device__ void chain_one(const ChainParams& p, SmemFor<KPM>& sm, double* wgt, int64_t s) {
     const int tid = threadIdx.x;
     const int64_t g = p.dp[s];
     bool ok = g >= 0 && g < p.G;
@@ -1065,13 +1114,13 @@ __device__ void chain_one(const ChainParams& p, Smem& sm, double* wgt, int64_t s
     }
 }
 
-__host__ __device__ constexpr size_t smem_fixed_bytes() { return (sizeof(Smem) + 15) & ~(size_t)15; }
 
 template <int TPL, int KPM, bool MIXED>
 __global__ void __launch_bounds__(PE_MAXT, PE_MINB) fock_chain_kernel(ChainParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
-    double* wgt = reinterpret_cast<double*>(smem_raw + smem_fixed_bytes());
+    using SM = SmemFor<KPM>;
+    SM& sm = *reinterpret_cast<SM*>(smem_raw);
+    double* wgt = reinterpret_cast<double*>(smem_raw + smem_fixed_bytes<KPM>());
     const int tid = threadIdx.x;
     for (;;) {
         if (tid == 0) {
@@ -1107,7 +1156,8 @@ struct SplitParams {
 
 // Stream state of step k from global memory into shared memory; false when the stream has fewer photons
 // than k (nothing to do) or an index is out of range (recorded).  Uniform across the CTA.
-static __device__ bool load_state(const ChainParams& p, Smem& sm, int64_t s, int k, int& m, int64_t& off) {
+template <class SM>
+static __device__ bool load_state(const ChainParams& p, SM& sm, int64_t s, int k, int& m, int64_t& off) {
     const int tid = threadIdx.x;
     if (tid == 0) { sm.bad = 0; sm.ngrp = 0; }
     __syncthreads();
@@ -1144,7 +1194,8 @@ static __device__ bool load_state(const ChainParams& p, Smem& sm, int64_t s, int
 template <int TPL, int KPM, bool MIXED>
 __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_partial_kernel(SplitParams sp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+    using SM = SmemFor<KPM>;
+    SM& sm = *reinterpret_cast<SM*>(smem_raw);
     const ChainParams& p = sp.c;
     const int tid = threadIdx.x, k = sp.k;
     for (int64_t item = blockIdx.x; item < p.S * sp.nch; item += gridDim.x) {
@@ -1168,8 +1219,9 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_partial_kernel(SplitPa
 template <int TPL, int KPM, bool MIXED>
 __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_draw_kernel(SplitParams sp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
-    double* wgt = reinterpret_cast<double*>(smem_raw + ((sizeof(Smem) + 15) & ~(size_t)15));
+    using SM = SmemFor<KPM>;
+    SM& sm = *reinterpret_cast<SM*>(smem_raw);
+    double* wgt = reinterpret_cast<double*>(smem_raw + smem_fixed_bytes<KPM>());
     const ChainParams& p = sp.c;
     const int tid = threadIdx.x, k = sp.k;
     for (int64_t s = blockIdx.x; s < p.S; s += gridDim.x) {
@@ -1224,7 +1276,8 @@ __global__ void __launch_bounds__(256) cofactor_kernel(const double2* __restrict
                                                        int64_t S, int m, int K, double2* __restrict__ P,
                                                        int* status, long long* detail) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    Smem& sm = *reinterpret_cast<Smem*>(smem_raw);
+    using SM = SmemFor<KPM>;
+    SM& sm = *reinterpret_cast<SM*>(smem_raw);
     const int tid = threadIdx.x;
     for (int64_t s = blockIdx.x; s < S; s += gridDim.x) {
         if (tid == 0) { sm.bad = 0; sm.ngrp = 0; sm.lane0 = 0; sm.lane_mult = 1; }

@@ -15,6 +15,7 @@ constexpr int WMID = 128;      // middle schedule length
 constexpr int WARPS = 8;       // warps (streams in flight) per CTA
 
 struct WarpSmem {
+    static constexpr int NKMAX = WMAXN;
     Plan plan;
     double2 P[WMAXN];
     double2 B[WMAXN][WMAXN];

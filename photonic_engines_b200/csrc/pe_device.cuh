@@ -6,7 +6,8 @@
 
 namespace pe {
 
-constexpr int MAXN = 32;        // photons per stream = largest cofactor tier (columns)
+constexpr int MAXN = 64;        // photons per stream = largest cofactor tier (columns)
+constexpr int NARROW = 32;      // tiers up to this many columns keep 32-wide shared-memory tables
 constexpr int LIN_MAX = 512;    // inner Gray block: terms walked from the shared inner schedule
 constexpr int MID_MAX = 1024;   // middle Gray block: inner blocks walked from the shared middle schedule
 constexpr int MAX_WARPS = 8;    // CTA of at most 256 threads
@@ -64,42 +65,49 @@ static __device__ __forceinline__ double signed_binom(int M, int v) {
 // inner digits are walked from the shared inner schedule (one CTA-uniform transition per term),
 // middle digits from the shared middle schedule once per inner block, high digits index the Gray
 // lanes (each lane owns one combination of them), fixed digits have radix 1.
-struct Plan {
+template <int NK>
+struct PlanT {
+    static constexpr int NKMAX = NK;   // largest number of columns (and of row groups + 1) it holds
     int64_t N;          // terms of the collapsed sum (the reference's addend count)
     int64_t H;          // lanes = product of high radices
     int Lin, Lmid;      // inner / middle combinations
     int K, K1, D;       // columns, chosen rows, digits (distinct chosen rows)
     int nin, nmid, nhi;
     double scale;       // 2^-K1, doubled when an odd group is halved
-    int R[MAXN];        // radix per kernel digit
-    int M[MAXN];        // multiplicity per kernel digit
-    int drow[MAXN];     // output mode per kernel digit
-    int Pin[MAXN];      // prefix products of the inner radices
-    int Pmid[MAXN];     // prefix products of the middle radices
-    unsigned char vend[MAXN];   // inner digit values after a forward inner block
-    int sortR[MAXN];    // scratch of the planner: active digits by ascending radix
-    int sortG[MAXN];
+    int R[NK];        // radix per kernel digit
+    int M[NK];        // multiplicity per kernel digit
+    int drow[NK];     // output mode per kernel digit
+    int Pin[NK];      // prefix products of the inner radices
+    int Pmid[NK];     // prefix products of the middle radices
+    unsigned char vend[NK];   // inner digit values after a forward inner block
+    int sortR[NK];    // scratch of the planner: active digits by ascending radix
+    int sortG[NK];
 };
 
-struct Smem {
-    Plan plan;
-    double2 P[MAXN];               // cofactors of the step (scaled)
-    double2 B[MAXN][MAXN];         // B[kd][j] = A[drow_kd, col_j], padded columns zero
-    alignas(16) float2 B32[MAXN][MAXN];   // 2 * B in float32 (the mixed form's Gray update); paired
+// Shared memory of one CTA working on one stream, for tiers of up to NK columns (32: the narrow layout
+// of chains up to 32 photons; 64: the wide one, FP64 only, so its FP32 copy of B is a placeholder).
+template <int NK>
+struct SmemT {
+    static constexpr int NKMAX = NK;
+    static constexpr int NK32 = NK <= NARROW ? NK : 1;
+    PlanT<NK> plan;
+    double2 P[NK];                 // cofactors of the step (scaled)
+    double2 B[NK][NK];             // B[kd][j] = A[drow_kd, col_j], padded columns zero
+    alignas(16) float2 B32[NK32][NK32];   // 2 * B in float32 (the mixed form's Gray update); paired
                                    // sweeps read each row as float4 slots (see prepare_step)
     double tab_w[LIN_MAX];         // inner weight prod (-1)^v C(M, v) at inner index t
     float tab_w32[LIN_MAX];
     double tab_wm[MID_MAX];        // middle weight at middle index
     unsigned char tab_f[LIN_MAX];  // transition into inner index t: digit | 0x80 when the update is -2 b
     unsigned char tab_fm[MID_MAX]; // transition into middle index: middle digit | 0x80 when -2 b
-    double2 red[MAX_WARPS][MAXN];  // cross-warp reduction
+    double2 red[MAX_WARPS][NK];  // cross-warp reduction
     double scan[MAX_WARPS];
     double fmin[MAX_WARPS];
     int cnt[MAX_WARPS];
-    int rows[MAXN];                // chosen modes so far
-    int cols[MAXN];                // input columns of the stream in chain order
-    int grow[MAXN];                // distinct chosen modes (groups), in order of first appearance
-    int gmul[MAXN];                // their multiplicities
+    int rows[NK];                // chosen modes so far
+    int cols[NK];                // input columns of the stream in chain order
+    int grow[NK];                // distinct chosen modes (groups), in order of first appearance
+    int gmul[NK];                // their multiplicities
     int ngrp;
     int64_t cur;                   // stream being processed (-1: queue drained)
     int64_t lane0;                 // this CTA's first Gray lane (split steps: chunk * lanes)
@@ -107,5 +115,17 @@ struct Smem {
     double tot, target;
     int bad;                       // set by any thread that saw an out-of-range index
 };
+
+using Plan = PlanT<NARROW>;
+using Smem = SmemT<NARROW>;
+template <int KPM>
+using SmemFor = SmemT<(KPM <= NARROW ? NARROW : MAXN)>;
+
+// Dynamic shared memory of a chain CTA before its m weights: the layout of the tier, 16-byte rounded.
+template <int KPM>
+__host__ __device__ constexpr size_t smem_fixed_bytes() { return (sizeof(SmemFor<KPM>) + 15) & ~(size_t)15; }
+__host__ __device__ constexpr size_t smem_fixed_bytes_for(int kpm) {
+    return kpm <= NARROW ? smem_fixed_bytes<NARROW>() : smem_fixed_bytes<MAXN>();
+}
 
 }  // namespace pe
