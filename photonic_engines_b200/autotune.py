@@ -19,7 +19,7 @@ CANDIDATES = {8: [(1, 128), (1, 256), (2, 128), (2, 256)],
               24: [(2, 64), (2, 128), (4, 128), (4, 256)],
               28: [(2, 64), (2, 128), (4, 128), (4, 256)],
               32: [(2, 64), (2, 128), (4, 128), (4, 256)],
-              40: [(4, 64), (4, 128)], 48: [(4, 64), (4, 128)], 56: [(4, 64), (4, 128)],
+              40: [(2, 64), (2, 128), (4, 128)], 48: [(4, 64), (4, 128)], 56: [(4, 64), (4, 128)],
               64: [(4, 64), (4, 128)]}
 
 

@@ -26,14 +26,14 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.
 # (mixed, threads per lane, largest tier) of every compiled chain/cofactor kernel pair
 VARIANTS = [(mx, tpl, kpm) for mx in (0, 1) for tpl, kpms in ((1, (8, 16, 20)), (2, (8, 16, 20, 24, 28, 32)),
                                                               (4, (8, 16, 20, 24, 28, 32))) for kpm in kpms]
-VARIANTS += [(0, 4, kpm) for kpm in (40, 48, 56, 64)]          # beyond 32 photons: FP64, four-thread lanes
+VARIANTS += [(0, 2, 40)] + [(0, 4, kpm) for kpm in (40, 48, 56, 64)]      # beyond 32 photons: FP64 only
 if os.environ.get("PE_VARIANTS"):          # a subset "m,t,k;m,t,k" (experiments: smaller, faster builds)
     VARIANTS = [tuple(int(x) for x in v.split(",")) for v in os.environ["PE_VARIANTS"].split(";")]
 
 
 def variant_flags(mx: int, tpl: int, kpm: int) -> list[str]:
     """Lanes that hold many columns per thread (one-thread lanes of 16 and 20 columns, two-thread lanes of
-    24 to 32, four-thread lanes of 40 to 64) are compiled for 128-thread CTAs, two per SM, so that every
+    24 to 40, four-thread lanes of 40 to 64) are compiled for 128-thread CTAs, two per SM, so that every
     thread may use 255 registers;
     the others for 256-thread CTAs at 128 registers.  Two-thread lanes at 24-32 columns compiled this way
     run 1.1-1.9x faster than four-thread lanes at 128 registers (FP64, m = 2n)."""

@@ -75,10 +75,10 @@ def default_tpl(n: int, precision: str) -> int:
     kpm = next((k for k in (8, 16, 20, 24, 28, 32, 40, 48, 56, 64) if n <= k), 64)
     if kpm <= 8 or (precision == "f64" and kpm == 20):
         return 1
-    return 2 if kpm <= 32 else 4
+    return 2 if kpm <= 40 else 4
 
 
-NCH_MAX = 64                 # CTAs per stream at most
+NCH_MAX = 512                # CTAs per stream at most
 
 
 @functools.lru_cache(maxsize=None)
@@ -96,8 +96,8 @@ def split_plan(heavy_streams: int, n: int, device, block_threads: int = 0, tpl: 
 
     nch is a power of two (a step's Gray lanes come in powers of two, so any other count leaves lanes idle)
     with heavy_streams * nch at least six times the split kernel's resident CTAs (`pe_split_slots`), so
-    that the last partial wave costs little (at most 64); of nch and 2 nch the one that fills its waves
-    better (by more than 2 %) wins.  k_split is the first step with enough Gray terms (2^(k-2)) for every
+    that the last partial wave costs little; at most 512, and at most what leaves the last four steps split
+    (2^(n-2) / (32 lanes)); of nch and 2 nch the one that fills its waves better (by more than 2 %) wins.  k_split is the first step with enough Gray terms (2^(k-2)) for every
     CTA to run several lanes.  The reference's single-sample path sizes a fixed lane grid instead
     (photonic_engines/clifford/single.py:22-82)."""
     if n < 8 or heavy_streams < 1:
@@ -114,14 +114,16 @@ def split_plan(heavy_streams: int, n: int, device, block_threads: int = 0, tpl: 
         items = heavy_streams * c
         return items / (-(-items // slots) * slots)
 
-    nch = 1
-    while nch < NCH_MAX and heavy_streams * nch < 6 * slots:
-        nch *= 2
-    if 2 * nch <= NCH_MAX and fill(2 * nch) > fill(nch) + 0.02:
-        nch *= 2
     lanes = block // max(tpl, 1)
-    while nch > 1 and (1 << (n - 2)) < 4 * nch * lanes:      # the last step must still be split
-        nch //= 2
+    # at most enough CTAs for the last four steps to be split (short chains: earlier steps stay whole)
+    cap = max(1, min(NCH_MAX, (1 << (n - 2)) // (32 * lanes)))
+    nch = 1
+    while nch < cap and heavy_streams * nch < 6 * slots:
+        nch *= 2
+    if 2 * nch <= cap and fill(2 * nch) > fill(nch) + 0.02:
+        nch *= 2
+    if nch == 1:
+        return None
     k = 2
     while k <= n and (1 << (k - 2)) < 4 * nch * lanes:
         k += 1

@@ -65,11 +65,11 @@ void* find_cofactor_kernel(int mixed, int tpl, int kpm) {
 // Threads per Gray lane when the caller passes 0 (measured at m = 400, 2 000 streams, and at m = 2n for
 // 21-32 photons): one-thread lanes up to 8 columns, and for FP64 chains of 17-20 photons (no exchange of
 // partial products; those variants run 128-thread CTAs with 255 registers); two-thread lanes beyond
-// (at 24-32 columns also compiled for 128-thread CTAs with 255 registers).
+// (at 24-40 columns compiled for 128-thread CTAs with 255 registers), four-thread lanes at 48-64.
 static int default_tpl(int kpm, int precision) {
     if (kpm <= 8) return 1;
     if (precision == PE_PRECISION_F64 && kpm == 20) return 1;
-    return kpm <= NARROW ? 2 : 4;
+    return kpm <= 40 ? 2 : 4;
 }
 
 static thread_local cudaError_t g_last_cuda_error = cudaSuccess;
@@ -460,7 +460,7 @@ extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t
     const int kpm = kpm_for(K);
     if (kpm < 0) return PE_ERR_SIZE;
     if (kpm > NARROW && precision != PE_PRECISION_F64) return PE_ERR_SIZE;
-    if (tpl == 0) tpl = kpm <= 8 ? 1 : (kpm <= NARROW ? 2 : 4);
+    if (tpl == 0) tpl = kpm <= 8 ? 1 : (kpm <= 40 ? 2 : 4);
     if (tpl_index(tpl) < 0) return PE_ERR_ARG;
     void* fn = find_cofactor_kernel(precision, tpl, kpm);
     if (!fn) return PE_ERR_SIZE;

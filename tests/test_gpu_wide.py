@@ -1,5 +1,5 @@
-"""Chains of 33 to 64 photons on the GPU (the wide tiers: 40, 48, 56 and 64 columns, FP64, four-thread
-lanes, 64-wide shared-memory tables), through the C ABI.
+"""Chains of 33 to 64 photons on the GPU (the wide tiers: 40, 48, 56 and 64 columns, FP64, two-thread
+lanes at 40 and four-thread lanes beyond, 64-wide shared-memory tables), through the C ABI.
 
 The oracle finishes such chains in seconds only when few distinct rows are chosen (the term count is the
 product of multiplicity + 1 over the distinct rows), so the chains run in few modes: picks bit-exact with
@@ -21,9 +21,9 @@ pytestmark = pytest.mark.gpu
 DEV = "cuda"
 
 
-@pytest.mark.parametrize(("n", "m", "split"), [(36, 8, False), (36, 8, None), (44, 7, False), (48, 6, None),
-                                               (64, 5, False)])
-def test_wide_chains_match_the_oracle(n, m, split):
+@pytest.mark.parametrize(("n", "m", "split", "tpl"), [(36, 8, False, 0), (36, 8, None, 4), (44, 7, False, 0),
+                                                      (48, 6, None, 0), (64, 5, False, 0)])
+def test_wide_chains_match_the_oracle(n, m, split, tpl):
     """Every step of the GPU's chains against the long-double oracle's step on the same history: the
     marginal within 50x the FP64 oracle's own distance from long double at that step (high multiplicities
     cancel: at k = 64 in 5 modes FP64 keeps ~3 digits), the pick equal wherever the draw is farther than
@@ -32,7 +32,7 @@ def test_wide_chains_match_the_oracle(n, m, split):
     U, sig, u = _random_chains(n, m, S, 900 + n)
     in_modes = [i % m for i in range(n)]                      # n photons in m < n input modes
     A = U[:, in_modes]
-    out = sample_chains(torch.tensor(U, device=DEV), in_modes, sig, uniforms=u, want_marg=True, split=split)
+    out = sample_chains(torch.tensor(U, device=DEV), in_modes, sig, uniforms=u, want_marg=True, split=split, tpl=tpl)
     rows, mg = out["rows"].cpu().numpy(), out["marg"].cpu().numpy()
     exact = 0
     for s in range(S):
