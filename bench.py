@@ -31,7 +31,7 @@ N_PHOT, M_MODES, SHOTS, USEED = 20, 400, 2000, 1002
 # DRAM bytes (read + write) of one chain launch on this workload, from one ncu capture of each form
 # (dram__bytes_read.sum + dram__bytes_write.sum, `--profile-launch f64|mixed`); the algorithmic bytes
 # (16 m k + 16 k^2 per sample and step, 2.78 GB per launch) are served from L2 and shared memory.
-DRAM_BYTES_PER_LAUNCH = {"f64": 1.038e6 + 0.067e6, "mixed": 1.908e6 + 0.177e6}
+DRAM_BYTES_PER_LAUNCH = {"f64": 1.119e6 + 0.0, "mixed": 1.008e6 + 0.023e6}
 METRIC = "samples/s n=20 m=400: mixed-precision vs FP64 on B200, marginal err<=1e-6"
 WORKLOAD = "fock n=20 photons (modes 0..19), m=400, 2000 shots/step, lossless, Haar U (seeded QR)"
 
