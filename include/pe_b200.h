@@ -118,6 +118,24 @@ int pe_fock_chain_warp(int precision, const double* d_acol, const int64_t* d_ins
                        int marg_stride, void* d_workspace, size_t workspace_bytes, int tpl, int grid_ctas,
                        void* stream);
 
+/*
+ * One tier of a length-sorted batch: as pe_fock_chain (warp = 0) or pe_fock_chain_warp (warp = 1), but the
+ * persistent queue runs only d_order[lo .. hi) with d_qrange = {lo, hi} read ON THE DEVICE (so a captured
+ * CUDA graph replays it for every batch), and the kernel is chosen for chains of at most nk_max photons
+ * (nk_max <= n_stride; a stream of the range with more is reported through the status word).  Launching
+ * the tiers of one batch — e.g. nk > 20, 17..20 and <= 16 with the warp form — on separate streams, each
+ * with its own workspace, runs every chain in the smallest kernel that holds it.  d_order and d_nk are
+ * required.  No counterpart in the reference (its batched kernels take one lane plan per launch,
+ * photonic_engines/clifford/cofactors_triton.py:450-465).
+ */
+int pe_fock_chain_range(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
+                        const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
+                        const int32_t* d_nk, const int64_t* d_cols, int n_stride, const double* d_uniforms,
+                        const int64_t* d_seeds, const int64_t* d_seed_row, const int64_t* d_rng_off,
+                        const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
+                        int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
+                        int grid_ctas, const int64_t* d_qrange, int nk_max, int warp, void* stream);
+
 /* Bytes of device workspace pe_fock_chain_split needs for S streams and nch CTAs per stream. */
 size_t pe_chain_split_workspace_bytes(int64_t S, int nch);
 

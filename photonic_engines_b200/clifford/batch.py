@@ -19,7 +19,7 @@ import torch
 
 from .. import _native as N
 from .. import autotune
-from .kernels import default_tpl, pack_ragged, split_plan, use_warp_form
+from .kernels import WARP_MAX_PHOTONS, default_tpl, pack_ragged, split_plan, use_warp_form
 
 
 def _per_instance(v, G, default):
@@ -38,11 +38,12 @@ class BatchedSampler:
     circuits: [(U_g [m_g, m_g] complex CUDA tensor, in_modes_g)], shots: int or per-circuit list,
     loss: transmission eta (scalar or per circuit), indist: x-model overlap x (scalar or per circuit),
     precision: "f64" | "mixed", seed: seeds the device generator, graph: capture the batch in a CUDA graph,
-    tune: pick the launch shape with the autotuner (cached per GPU and workload).
+    tune: pick the launch shape with the autotuner (cached per GPU and workload); tiers: run chains of
+    different lengths in kernels sized to them (False: one launch sized to the longest).
     """
 
     def __init__(self, circuits, shots, loss=None, indist=None, precision: str = "mixed", seed: int = 0,
-                 graph: bool = True, tune: bool = True, block_threads: int = 0, tpl: int = 0):
+                 graph: bool = True, tune: bool = True, block_threads: int = 0, tpl: int = 0, tiers: bool = True):
         if not circuits:
             raise ValueError("at least one circuit")
         if precision not in N.PRECISIONS:
@@ -100,6 +101,20 @@ class BatchedSampler:
                                   device=dev)
         else:
             self.ws = N.workspace(dev)
+        # length tiers: when the chains of a batch differ in length (loss, singles, circuits of several n),
+        # every chain runs in the smallest kernel that holds it — the length-sorted order is cut on the device
+        # into > 20, 17..20 and <= 16 photons (the last in the warp form), one launch per tier on its own
+        # stream with its own workspace (pe_fock_chain_range), so the graph replays the cut for every batch
+        varied = self.singles or any(e < 1.0 for e in etas) or len(set(self.n)) > 1
+        self.tiers = []
+        if tiers and varied and not self.warp and not self.split and self.n_stride > WARP_MAX_PHOTONS:
+            self.tiers = [(self.n_stride, 0)] + ([(20, 0)] if self.n_stride > 20 else []) + [(WARP_MAX_PHOTONS, 1)]
+            self.tier_thr = torch.tensor([t[0] for t in self.tiers[1:]], dtype=torch.int32, device=dev)
+            self.qr = torch.zeros(len(self.tiers), 2, dtype=torch.int64, device=dev)
+            self.qr[-1, 1] = C                                           # the cuts between tiers move per batch
+            wsb = int(N.load().pe_chain_workspace_bytes(C))
+            self.tier_ws = [torch.zeros(wsb, dtype=torch.uint8, device=dev) for _ in self.tiers]
+            self.tier_streams = [torch.cuda.Stream(dev) for _ in self.tiers[1:]]
         self.gen = torch.Generator(device=dev).manual_seed(seed)
         self._row0 = [0]
         for s_ in shots_l:
@@ -135,6 +150,22 @@ class BatchedSampler:
                   self.m_max, None, self.m_max)
         block = int(self.block if block is None else block)
         tpl = int(self.tpl if tpl is None else tpl)
+        if self.tiers:
+            cnt = (self.nk_sorted.unsqueeze(0) > self.tier_thr.unsqueeze(1)).sum(1)    # chains above each cut
+            self.qr[1:, 0] = cnt
+            self.qr[:-1, 1] = cnt
+            cur = torch.cuda.current_stream(self.device)
+            for s_ in self.tier_streams:
+                s_.wait_stream(cur)
+            for i, (nk_max, warp) in enumerate(self.tiers):
+                stream = cur if i == 0 else self.tier_streams[i - 1]
+                b, t = (block, tpl) if i == 0 else (0, 0)          # the tuned shape is the top tier's
+                rc = L.pe_fock_chain_range(*common, N.ptr(self.tier_ws[i]), self.tier_ws[i].numel(), b, t, 0,
+                                           N.ptr(self.qr[i]), nk_max, warp, stream.cuda_stream)
+                N.check(rc, "pe_fock_chain_range")
+            for s_ in self.tier_streams:
+                cur.wait_stream(s_)
+            return
         if self.warp:
             rc = L.pe_fock_chain_warp(*common, N.ptr(self.ws), self.ws.numel(), tpl if tpl in (1, 2) else 0, 0, st)
         elif self.split:
@@ -158,7 +189,7 @@ class BatchedSampler:
 
     def _autotune(self):
         workload = (f"batch|G{self.G}|S{self.S}|m{self.m_max}|n{self.n_stride}|singles{int(self.singles)}|"
-                    f"{'warp' if self.warp else 'cta'}")
+                    f"{'warp' if self.warp else 'cta'}|tiers{len(self.tiers)}")
         self._draw_keys()
         self._partition()
         best = autotune.tune(lambda tpl, block: self._chains(tpl, block), self.device, self.precision,
@@ -196,7 +227,9 @@ class BatchedSampler:
     def check(self) -> None:
         """Raise when a device-side index error was recorded (synchronises)."""
         st = self.status.cpu().tolist()
-        ws, _ = N.read_status(self.ws)
+        ws = 0
+        for w in (self.tier_ws if self.tiers else [self.ws]):
+            ws = ws or N.read_status(w)[0]
         if any(st) or ws:
             raise N.NativeError(f"device-side error in the batched sampler (partition {st[0]}, scatter {st[1]}, "
                                 f"chains {ws})")

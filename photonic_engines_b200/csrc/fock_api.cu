@@ -252,8 +252,10 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
                         const int64_t* d_order, int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
                         int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
                         int grid_ctas, int k_split, int nch, void* stream, bool warp_mode = false,
-                        int k_first = 1, int k_last = 0, bool zero_status = true) {
+                        int k_first = 1, int k_last = 0, bool zero_status = true,
+                        const int64_t* d_qrange = nullptr, int nk_max = 0) {
     if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
+    if (nk_max < 0 || nk_max > n_stride || (d_qrange && k_split > 0)) return PE_ERR_ARG;
     if (k_first < 1 || k_first > n_stride + 1 || k_last < 0) return PE_ERR_ARG;
     if (S < 0 || G < 1 || m_max < 1 || n_stride < 1) return PE_ERR_ARG;
     if (!d_acol || !d_inst_off || !d_inst_m || !d_inst_n || !d_dp || !d_cols || !d_rows || !d_workspace) return PE_ERR_ARG;
@@ -265,7 +267,8 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     const size_t part_bytes = split ? (size_t)S * nch * MAXN * sizeof(double2) : 0;
     const size_t need = WS_BYTES + part_bytes + (split ? (size_t)S * sizeof(int) : 0);
     if (workspace_bytes < need || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
-    const int kpm = kpm_for(n_stride);
+    const int ncols = nk_max > 0 ? nk_max : n_stride;        // the longest chain the launch may meet
+    const int kpm = kpm_for(ncols);
     if (kpm < 0) return PE_ERR_SIZE;
     if (kpm > NARROW && precision != PE_PRECISION_F64) return PE_ERR_SIZE;   // mixed form: up to 32 columns
     if (warp_mode && (kpm > WMAXN || split)) return PE_ERR_SIZE;
@@ -281,7 +284,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     // default CTA: 128 threads (as many warps per SM as 256-thread CTAs, twice the CTAs to overlap the
     // per-step serial phases of one stream with the sweeps of others)
     const int block = warp_mode ? 32 * WARPS : (block_threads ? block_threads : (bmax < 128 ? bmax : 128));
-    if (block < 32 || block > 256 || block > bmax || (block & 31) || block < n_stride) return PE_ERR_ARG;
+    if (block < 32 || block > 256 || block > bmax || (block & 31) || block < ncols) return PE_ERR_ARG;
     const size_t smem = warp_mode ? warp_smem_bytes() : smem_fixed_bytes_for(kpm) + (size_t)m_max * sizeof(double);
     const int cap = max_smem_optin();
     if (cap <= 0) return PE_ERR_CUDA;
@@ -305,6 +308,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     p.inst_off = d_inst_off; p.inst_m = d_inst_m; p.inst_n = d_inst_n; p.G = G;
     p.S = S; p.dp = d_dp; p.nk = d_nk; p.cols = d_cols; p.n_stride = n_stride;
     p.uniforms = d_uniforms; p.seeds = d_seeds; p.seed_row = d_seed_row; p.rng_off = d_rng_off; p.order = d_order;
+    p.qrange = d_qrange;
     p.rows = d_rows; p.occ = d_occ; p.occ_stride = d_occ ? occ_stride : m_max; p.marg = d_marg; p.marg_stride = marg_stride;
     p.queue = (unsigned long long*)d_workspace;
     p.status = (int*)((char*)d_workspace + 8);
@@ -358,6 +362,21 @@ extern "C" int pe_fock_chain(int precision, const double* d_acol, const int64_t*
     return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, d_nk, d_cols, n_stride,
                         d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ, occ_stride, d_marg,
                         marg_stride, d_workspace, workspace_bytes, block_threads, tpl, grid_ctas, 0, 1, stream);
+}
+
+extern "C" int pe_fock_chain_range(int precision, const double* d_acol, const int64_t* d_inst_off,
+                                   const int32_t* d_inst_m, const int32_t* d_inst_n, int G, int m_max, int64_t S,
+                                   const int64_t* d_dp, const int32_t* d_nk, const int64_t* d_cols, int n_stride,
+                                   const double* d_uniforms, const int64_t* d_seeds, const int64_t* d_seed_row,
+                                   const int64_t* d_rng_off, const int64_t* d_order, int64_t* d_rows, int64_t* d_occ,
+                                   int occ_stride, double* d_marg, int marg_stride, void* d_workspace,
+                                   size_t workspace_bytes, int block_threads, int tpl, int grid_ctas,
+                                   const int64_t* d_qrange, int nk_max, int warp, void* stream) {
+    if (!d_qrange || !d_order || !d_nk || nk_max < 1 || (warp != 0 && warp != 1)) return PE_ERR_ARG;
+    return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, d_nk, d_cols, n_stride,
+                        d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ, occ_stride, d_marg,
+                        marg_stride, d_workspace, workspace_bytes, warp ? 0 : block_threads, tpl, grid_ctas, 0, 1,
+                        stream, warp == 1, 1, 0, true, d_qrange, nk_max);
 }
 
 extern "C" int pe_fock_chain_warp(int precision, const double* d_acol, const int64_t* d_inst_off,

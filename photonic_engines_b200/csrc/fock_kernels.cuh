@@ -64,6 +64,8 @@ struct ChainParams {
     const int64_t* seed_row;
     const int64_t* rng_off;
     const int64_t* order;
+    const int64_t* qrange;  // optional [2] on the device: the queue runs order[lo .. hi) only (a tier of a
+                            // length-sorted batch); null: the whole [0, S)
     int64_t* rows;
     int64_t* occ;
     int occ_stride;
@@ -87,6 +89,26 @@ constexpr int MIXED_LIN = PE_MIXED_LIN;
 
 // Workspace layout: [0] queue counter (u64), [8] status (i32), [16] detail (i64).  Zeroed per call.
 constexpr size_t WS_BYTES = 256;
+
+static __device__ __forceinline__ void record_error(int* status, long long* detail, int64_t s);
+
+// The stream that queue ticket q stands for: order[lo + q] over the range [lo, hi) of the queue (qrange,
+// or the whole [0, S)); -1 once the range is drained.  An invalid range counts as empty and is recorded
+// (detail S).
+static __device__ __forceinline__ int64_t queue_stream(const ChainParams& p, unsigned long long q) {
+    int64_t lo = 0, hi = p.S;
+    if (p.qrange) {
+        lo = p.qrange[0];
+        hi = p.qrange[1];
+        if (lo < 0 || hi > p.S || lo > hi) {
+            if (q == 0) record_error(p.status, p.detail, p.S);
+            return -1;
+        }
+    }
+    const int64_t idx = lo + (int64_t)q;
+    if (q >= (unsigned long long)(hi - lo)) return -1;
+    return p.order ? p.order[idx] : idx;
+}
 
 static __device__ __forceinline__ void record_error(int* status, long long* detail, int64_t s) {
     if (atomicCAS(status, 0, PE_ERR_DEVICE) == 0) *detail = (long long)s;
@@ -1124,8 +1146,7 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) fock_chain_kernel(ChainParam
     const int tid = threadIdx.x;
     for (;;) {
         if (tid == 0) {
-            const unsigned long long q = atomicAdd(p.queue, 1ull);
-            sm.cur = (q < (unsigned long long)p.S) ? (p.order ? p.order[q] : (int64_t)q) : -1;
+            sm.cur = queue_stream(p, atomicAdd(p.queue, 1ull));
             sm.bad = 0;
         }
         __syncthreads();

@@ -326,8 +326,7 @@ __global__ void __launch_bounds__(32 * WARPS, 2) fock_chain_warp_kernel(ChainPar
     const int lane = threadIdx.x & 31;
     for (;;) {
         if (lane == 0) {
-            const unsigned long long q = atomicAdd(p.queue, 1ull);
-            sm.cur = (q < (unsigned long long)p.S) ? (p.order ? p.order[q] : (int64_t)q) : -1;
+            sm.cur = queue_stream(p, atomicAdd(p.queue, 1ull));
         }
         __syncwarp();
         const int64_t s = sm.cur;

@@ -51,3 +51,17 @@ def test_indist_spec_normalisation():
         spec(1.5)
     with pytest.raises(ValueError):
         Distinguishability(x=0.5, species=(0.2,))
+
+
+def test_photon_limits_are_checked_on_the_host():
+    """64 photons in FP64, 32 in the mixed form (its FP32 error grows ~1.35x per column); the C ABI
+    answers PE_ERR_SIZE beyond them, the host refuses first with a clear message."""
+    N.check_photons(64, "f64")
+    N.check_photons(32, "mixed")
+    with pytest.raises(ValueError, match="at most 64"):
+        N.check_photons(65, "f64")
+    with pytest.raises(ValueError, match="mixed"):
+        N.check_photons(33, "mixed")
+    from photonic_engines_b200.clifford.kernels import default_tpl
+    assert [default_tpl(n, "f64") for n in (6, 18, 24, 32, 36, 48, 64)] == [1, 1, 2, 2, 2, 4, 4]
+    assert [default_tpl(n, "mixed") for n in (6, 18, 24, 32)] == [1, 2, 2, 2]

@@ -104,3 +104,44 @@ def test_graph_and_eager_paths_agree_in_law():
         bs = BatchedSampler(circ, 30000, loss=0.9, indist=0.8, seed=11, graph=graph, tune=False)
         tvd, floor = O.tvd_and_floor(dist, bs.sample().cpu().numpy())
         assert tvd < 2.5 * floor
+
+
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_length_tiers_give_the_single_launch_samples(precision):
+    """Lossy, partially distinguishable chains of up to 24 photons: the tiered launches (> 20, 17..20 and
+    <= 16 photons, the last in the warp form, on three streams) draw the samples of one launch sized to
+    the longest chain (same generator, same partition, same picks)."""
+    U = torch.tensor(O.haar_unitary(48, 8), device=DEV)
+    circ = [(U, list(range(24)))]
+    out = []
+    for tiers in (True, False):
+        bs = BatchedSampler(circ, 3000, loss=0.7, indist=0.9, precision=precision, seed=5, tune=False, tiers=tiers)
+        assert bool(bs.tiers) == tiers
+        out.append((bs.sample().clone(), bs.sample().clone()))
+        bs.check()
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+
+
+def test_a_tier_reports_a_chain_longer_than_its_kernel_and_a_bad_range():
+    from photonic_engines_b200 import _native as N
+    from photonic_engines_b200.clifford.kernels import pack_instances
+    L = N.load()
+    U = torch.tensor(O.haar_unitary(40, 2), device=DEV)
+    n, S = 20, 4
+    acol, off, mm, nn = pack_instances(U, list(range(n)))
+    a2 = torch.view_as_real(acol.contiguous()) if acol.dtype != torch.float64 else acol
+    dp = torch.zeros(S, dtype=torch.int64, device=DEV)
+    cols = torch.arange(n, device=DEV).repeat(S, 1).contiguous()
+    nk = torch.tensor([18, 12, 10, 5], dtype=torch.int32, device=DEV)
+    order = torch.arange(S, device=DEV)
+    seeds = torch.arange(1, n + 1, device=DEV)[None].contiguous()
+    rows = torch.zeros(S, n, dtype=torch.int64, device=DEV)
+    for qr, nk_max in (([0, S], 16), ([3, 1], 20)):
+        qrange = torch.tensor(qr, dtype=torch.int64, device=DEV)
+        ws = N.workspace(torch.device(DEV))
+        rc = L.pe_fock_chain_range(0, N.ptr(a2), N.ptr(off), N.ptr(mm), N.ptr(nn), 1, 40, S, N.ptr(dp), N.ptr(nk),
+                                   N.ptr(cols), n, None, N.ptr(seeds), None, None, N.ptr(order), N.ptr(rows), None,
+                                   40, None, 40, N.ptr(ws), ws.numel(), 0, 0, 0, N.ptr(qrange), nk_max,
+                                   1 if nk_max <= 16 else 0, N.stream_handle(torch.device(DEV)))
+        assert rc == 0
+        assert N.read_status(ws)[0] == N.PE_ERR_DEVICE, (qr, nk_max)
