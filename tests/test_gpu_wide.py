@@ -1,5 +1,5 @@
 """Chains of 33 to 64 photons on the GPU (the wide tiers: 40, 48, 56 and 64 columns, FP64, two-thread
-lanes at 40 and four-thread lanes beyond, 64-wide shared-memory tables), through the C ABI.
+lanes at 40 and four-thread lanes at 40 and beyond, 64-wide shared-memory tables), through the C ABI.
 
 The oracle finishes such chains in seconds only when few distinct rows are chosen (the term count is the
 product of multiplicity + 1 over the distinct rows), so the chains run in few modes: picks bit-exact with
@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 DEV = "cuda"
 
 
-@pytest.mark.parametrize(("n", "m", "split", "tpl"), [(36, 8, False, 0), (36, 8, None, 4), (44, 7, False, 0),
+@pytest.mark.parametrize(("n", "m", "split", "tpl"), [(36, 8, False, 0), (38, 8, None, 4), (44, 7, False, 0),
                                                       (48, 6, None, 0), (64, 5, False, 0)])
 def test_wide_chains_match_the_oracle(n, m, split, tpl):
     """Every step of the GPU's chains against the long-double oracle's step on the same history: the
