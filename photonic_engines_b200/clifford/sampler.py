@@ -22,7 +22,7 @@ from dataclasses import dataclass
 import torch
 
 from .. import _native as N
-from ..imperfections import draw_roles, partition, route_classical, spec
+from ..imperfections import as_model, draw_fates, group_fates, route_lone_photons
 from .kernels import chain, chain_adaptive, default_tpl, pack_instances, split_plan
 from .prefix import prefix_order
 
@@ -111,7 +111,7 @@ def fock_sample(U, in_modes, shots, generator=None, algo="auto", multi_min_k1=10
     a stream is dropped as soon as one does, and only the survivors are returned ([S', m]; with keep_ids=True
     the pair (occupations, surviving stream ids)).  Both as the reference's sampler.py:26-39, 391-460.
     """
-    d = spec(indist)
+    d = as_model(indist)
     if prefix is not None:
         prefix = torch.as_tensor(prefix, dtype=torch.int64)
         if prefix.dim() == 2 and prefix.shape[0] == 1 and U.dim() == 2:
@@ -284,7 +284,7 @@ def plan_chains(U, in_modes, S: int, dp_all, generator, loss, indist, max_stream
         U = U[None]
     dev = U.device
     n = len(in_modes)
-    d = spec(indist)
+    d = as_model(indist)
     lossless = loss is None or float(loss) >= 1.0
     if lossless and d is None:
         sig, seeds, chunk, off = _pass_draws(S, n, generator, dev, max_streams)
@@ -295,7 +295,7 @@ def plan_chains(U, in_modes, S: int, dp_all, generator, loss, indist, max_stream
     by_cols: dict = {}                       # column tuple -> [stream ids]
     rep_sub: dict = {}                       # column tuple -> photon indices (columns of the packed instance)
     single_ids, single_cols = [], []
-    for subsets, singles, ids in partition(n, S, loss, d, generator=gen):
+    for subsets, singles, ids in group_fates(draw_fates(n, S, loss, d, generator=gen)):
         for sub in subsets:
             cols = tuple(int(in_modes[j]) for j in sub)
             if len(cols) == 1:
@@ -329,7 +329,7 @@ def plan_chains(U, in_modes, S: int, dp_all, generator, loss, indist, max_stream
     s_ids = s_rows = None
     if single_ids:                           # host draws after every pass has drawn (the reference's order)
         s_ids = torch.cat(single_ids).to(dev)
-        s_rows = route_classical(U, dp_all[s_ids].cpu(), torch.cat(single_cols), generator=gen).to(dev)
+        s_rows = route_lone_photons(U, dp_all[s_ids].cpu(), torch.cat(single_cols), generator=gen).to(dev)
     if not ch_dp:
         z = torch.zeros(0, dtype=torch.int64, device=dev)
         return ChainPlan(S, n, 0, z, z.reshape(0, n), z.to(torch.int32), z.reshape(0, n), z, z, z, z, s_ids, s_rows, [])
@@ -347,11 +347,11 @@ def _plan_loss_only(U, in_modes, S, dp_all, generator, gen, loss, max_streams) -
     sorted order, each group's streams in ascending order; one-photon groups are routed classically."""
     dev = U.device
     n = len(in_modes)
-    roles = draw_roles(n, S, loss, None, generator=gen)
-    # rows hold LOST (0) or 2 only, so their lexicographic order (torch.unique over rows) is the order of
+    fates = draw_fates(n, S, loss, None, generator=gen)
+    # rows hold LOST or species 0 only, so their lexicographic order (the grouping order) is the order of
     # the survival bitmask with photon 0 as the most significant bit: a 1-D unique gives the same groups
     weights = torch.tensor([1 << (n - 1 - j) for j in range(n)], dtype=torch.int64)
-    mask = ((roles == 2).to(torch.int64) * weights).sum(1)
+    mask = ((fates == 1).to(torch.int64) * weights).sum(1)
     umask, inv = torch.unique(mask, return_inverse=True)
     kept = ((umask[:, None] // weights[None, :]) % 2).bool()            # [G, n] surviving photons
     kg = kept.sum(1)                                                     # photons per group
@@ -395,7 +395,7 @@ def _plan_loss_only(U, in_modes, S, dp_all, generator, gen, loss, max_streams) -
         idx = idx[torch.sort(inv[idx], stable=True).indices]
         photon = torch.nonzero(kept[inv[idx]])[:, 1]
         s_ids = idx.to(dev)
-        s_rows = route_classical(U, dp_all[s_ids].cpu(), im_of(in_modes)[photon], generator=gen).to(dev)
+        s_rows = route_lone_photons(U, dp_all[s_ids].cpu(), im_of(in_modes)[photon], generator=gen).to(dev)
     if not ch_dp:
         z = torch.zeros(0, dtype=torch.int64, device=dev)
         return ChainPlan(S, n, 0, z, z.reshape(0, n), z.to(torch.int32), z.reshape(0, n), z, z, z, z, s_ids, s_rows, [])

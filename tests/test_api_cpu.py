@@ -7,7 +7,7 @@ from oracle import oracle as O
 from photonic_engines_b200 import FockState
 from photonic_engines_b200 import _native as N
 from photonic_engines_b200.clifford import fock_sample, sample
-from photonic_engines_b200.imperfections import Distinguishability, spec
+from photonic_engines_b200.imperfections import Distinguishability, as_model
 
 U4 = torch.as_tensor(O.haar_unitary(4, 13))
 
@@ -43,14 +43,18 @@ def test_sample_refuses_other_input_types():
     assert FockState((1, 0, 2)).modes() == [0, 2, 2]
 
 
-def test_indist_spec_normalisation():
-    assert spec(None) is None and spec(1.0) is None
-    assert spec(0.9) == Distinguishability(x=0.9)
-    assert spec([1.0, 0.8, 0.95]) == Distinguishability(x=0.8)
+def test_indist_model_normalisation():
+    assert as_model(None) is None and as_model(1.0) is None
+    assert as_model(0.9) == Distinguishability(x=0.9)
+    assert as_model([1.0, 0.8, 0.95]) == Distinguishability(x=0.8)
+    assert as_model(Distinguishability(species=(1.0,))) is None
+    assert Distinguishability.from_hom_visibility(0.81) == Distinguishability(x=0.9)
     with pytest.raises(ValueError):
-        spec(1.5)
+        as_model(1.5)
     with pytest.raises(ValueError):
         Distinguishability(x=0.5, species=(0.2,))
+    with pytest.raises(ValueError):
+        Distinguishability(species=(0.7, 0.4))
 
 
 def test_photon_limits_are_checked_on_the_host():
