@@ -268,6 +268,37 @@ def exact_distribution(U, in_modes) -> dict:
     return dist
 
 
+def imperfect_distribution(U, in_modes, eta: float, x: float) -> dict:
+    """Exact law of lossy, x-model partially distinguishable photons: every photon independently lost
+    (1 - eta), interfering (eta x) or alone (eta (1 - x)); the interfering ones follow the permanent law,
+    each lone one lands in row r with probability |U[r, col]|^2, and the occupations add (the model of
+    photonic_engines/imperfections.py, the reference's x_mixture in slos/species.py)."""
+    U = np.asarray(U, dtype=np.complex128)
+    m, n = U.shape[0], len(in_modes)
+    dist: dict = {}
+    for roles in itertools.product((0, 1, 2), repeat=n):        # 0 lost, 1 alone, 2 interfering
+        p = 1.0
+        for r in roles:
+            p *= (1 - eta) if r == 0 else (eta * (1 - x) if r == 1 else eta * x)
+        if p == 0.0:
+            continue
+        inter = [in_modes[j] for j in range(n) if roles[j] == 2]
+        lone = [in_modes[j] for j in range(n) if roles[j] == 1]
+        part = exact_distribution(U, inter) if inter else {tuple([0] * m): 1.0}
+        for col in lone:
+            w = np.abs(U[:, col]) ** 2
+            new: dict = {}
+            for k, q in part.items():
+                for r_ in range(m):
+                    kk = list(k)
+                    kk[r_] += 1
+                    new[tuple(kk)] = new.get(tuple(kk), 0.0) + q * w[r_]
+            part = new
+        for k, q in part.items():
+            dist[k] = dist.get(k, 0.0) + p * q
+    return dist
+
+
 def tvd_and_floor(dist: dict, occ) -> tuple[float, float]:
     """Total-variation distance of the empirical histogram of `occ` [S, m] to `dist`, and its
     shot-noise level 0.5 sum sqrt(p (1 - p) / S) sqrt(2 / pi) (tests/clifford/check_sampler.py:59-60)."""

@@ -2,7 +2,7 @@
 
 Run in a container where the reference project is importable (it is NOT needed at test time):
 
-    python tests/golden/make_golden.py /path/to/photonic-engines [philox steps chains adaptive emitter]
+    python tests/golden/make_golden.py /path/to/photonic-engines [philox steps chains adaptive emitter slos]
 
 It imports the reference read-only and records, with CPU tensors and the Triton CPU interpreter:
 
@@ -21,6 +21,8 @@ It imports the reference read-only and records, with CPU tensors and the Triton 
   emitter.npz  EmitterMPS inputs (chi = 2): step weights of `emitter_reference.matrix_cofactor_weights`
                (emitter_reference.py:280-305) and occupations drawn by the exact torch sampler
                `emitter_sampler.sample_torch` (emitter_sampler.py:82-180) for seeded CPU generators.
+  slos.npz     exact output probabilities of small circuits from the reference's SLOS kernel
+               (slos/kernel.py:83-285): lossless, bunched input, x-model and lossy cases.
   chains.npz   whole chains drawn by the reference's sampler: `_sample_streams`
                (sampler.py:391-460) rows [S, n] in chain order, plus the sigma and per-step seeds
                the generator produced, and `fock_sample` occupations with loss / partial
@@ -308,6 +310,41 @@ def make_emitter():
     np.savez_compressed(os.path.join(HERE, "emitter.npz"), **out)
 
 
+# (name, m, input modes, Haar seed, loss eta or None, x-model overlap or None): the small cases whose exact
+# law the tests compare samples with (histogram TVD tests), lossless, lossy and partially distinguishable
+SLOS_CASES = [("m4_n3", 4, [0, 1, 2], 104, None, None), ("m5_bunched", 5, [0, 0, 1], 105, None, None),
+              ("m6_n4", 6, [0, 1, 2, 3], 106, None, None), ("m5_n3_x07", 5, [0, 1, 2], 55, None, 0.7),
+              ("m4_n3_loss06", 4, [0, 1, 2], 5, 0.6, None)]
+
+
+def make_slos():
+    """slos.npz: exact output probabilities from the reference's SLOS kernel (FockSLOSKernel.probs,
+    photonic_engines/slos/kernel.py:83-285, complex128; `indist=` its x-mixture, `loss=` its thinned
+    LossyDistribution) on Haar circuits built as the oracle builds them (the oracle's haar_unitary, which
+    restates tests/helpers.py:10-17)."""
+    from photonic_engines.slos.kernel import FockSLOSKernel
+    sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+    from oracle.oracle import haar_unitary
+    out = {}
+    for name, m, modes, seed, eta, x in SLOS_CASES:
+        U = torch.as_tensor(haar_unitary(m, seed))
+        occ_in = [modes.count(j) for j in range(m)]
+        ker = FockSLOSKernel(len(modes), m, occ_in, dtype=torch.complex128)
+        if eta is not None:
+            d = ker.probs(U, loss=eta).as_dict()
+            states = np.array([list(k) for k in d], dtype=np.int64)
+            probs = np.array([float(v) for v in d.values()])
+        else:
+            probs = ker.probs(U, indist=x).numpy() if x is not None else ker.probs(U).numpy()
+            states = np.array(ker.layers.final_states, dtype=np.int64)
+        out[f"{name}__meta"] = np.array([m, seed, -1.0 if eta is None else eta, -1.0 if x is None else x])
+        out[f"{name}__modes"] = np.array(modes, dtype=np.int64)
+        out[f"{name}__states"] = states
+        out[f"{name}__probs"] = probs
+        print(name, "slos", states.shape, float(probs.sum()), flush=True)
+    np.savez_compressed(os.path.join(HERE, "slos.npz"), **out)
+
+
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PE_REFERENCE", "")
     if not ref or not os.path.isdir(ref):
@@ -316,5 +353,5 @@ if __name__ == "__main__":
     parts = sys.argv[2:] or ["philox", "steps", "chains", "adaptive"]
     for part in parts:
         {"philox": make_philox, "steps": make_steps, "chains": make_chains, "adaptive": make_adaptive,
-         "emitter": make_emitter}[part]()
+         "emitter": make_emitter, "slos": make_slos}[part]()
         print(part, "done", flush=True)

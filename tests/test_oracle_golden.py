@@ -94,3 +94,25 @@ def test_long_double_chain_agrees_with_the_fp64_chain():
     assert np.array_equal(a["rows"], b["rows"])
     assert np.abs(a["marg"] - b["marg"]).max() <= 1e-12
     assert np.array_equal(a["addends"], b["addends"])
+
+
+SLOS = np.load(os.path.join(GOLDEN, "slos.npz"))
+SLOS_CASES = sorted({k.split("__")[0] for k in SLOS.files})
+
+
+@pytest.mark.parametrize("name", SLOS_CASES)
+def test_exact_distributions_match_the_reference_slos(name):
+    """The oracle's exact output laws (Ryser enumeration; the lossy / x-model mixture) against the
+    probabilities of the reference's SLOS kernel on the same circuits: every outcome within 1e-12, the
+    same support.  These laws are the ones the histogram tests measure their TVD against."""
+    m, seed, eta, x = SLOS[f"{name}__meta"].tolist()
+    modes = SLOS[f"{name}__modes"].tolist()
+    U = O.haar_unitary(int(m), int(seed))
+    if eta < 0 and x < 0:
+        dist = O.exact_distribution(U, modes)
+    else:
+        dist = O.imperfect_distribution(U, modes, 1.0 if eta < 0 else eta, 1.0 if x < 0 else x)
+    ref = {tuple(int(v) for v in st): float(p) for st, p in zip(SLOS[f"{name}__states"], SLOS[f"{name}__probs"])}
+    keys = set(ref) | {k for k, p in dist.items() if p > 1e-15}
+    assert max(abs(dist.get(k, 0.0) - ref.get(k, 0.0)) for k in keys) <= 1e-12
+    assert abs(sum(ref.values()) - 1.0) <= 1e-12
