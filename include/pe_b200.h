@@ -48,9 +48,12 @@ extern "C" {
 
 #define PE_PRECISION_F64 0     /* complex FP64 throughout: the drop-in form */
 #define PE_PRECISION_MIXED 1   /* FP32 Gray blocks, FP64 cross-block sum, FP64 marginal and CDF */
+#define PE_PRECISION_COMPENSATED 2  /* FP32 Gray blocks in compensated double-float arithmetic (exact
+                                       on-grid column sums, TwoProduct / TwoSum products and block sums),
+                                       FP64 cross-block sum, marginal and CDF: FP64-level marginals */
 
 #define PE_MAX_PHOTONS 64      /* photons per stream (cofactor tiers up to 64 columns) */
-#define PE_MIXED_MAX_PHOTONS 32 /* the mixed form (FP32 Gray blocks) up to 32; FP64 beyond */
+#define PE_MIXED_MAX_PHOTONS 32 /* the mixed forms (FP32 Gray blocks) up to 32; FP64 beyond */
 
 /* Library version (major * 10000 + minor * 100 + patch). */
 int pe_version(void);
@@ -74,8 +77,9 @@ size_t pe_chain_workspace_bytes(int64_t S);
  *   photonic_engines/clifford/cuda_cofactors.py:278-299   cofactor_partials_cuda (cof_multi)
  *   photonic_engines/clifford/cofactors_triton.py:533-545 draw_step (_draw_kernel)
  *
- * precision: PE_PRECISION_F64 or PE_PRECISION_MIXED.  block_threads: 64, 128 or 256 (0 = default).
- * tpl: threads per Gray lane (1, 2 or 4; 0 = default).  grid_ctas: persistent CTAs (0 = occupancy).
+ * precision: PE_PRECISION_F64, PE_PRECISION_MIXED or PE_PRECISION_COMPENSATED.  block_threads: 64, 128
+ * or 256 (0 = default).  tpl: threads per Gray lane (1, 2 or 4; 0 = default).  grid_ctas: persistent
+ * CTAs (0 = occupancy).
  */
 int pe_fock_chain(int precision, const double* d_acol, const int64_t* d_inst_off, const int32_t* d_inst_m,
                   const int32_t* d_inst_n, int G, int m_max, int64_t S, const int64_t* d_dp,
@@ -119,7 +123,8 @@ int pe_fock_chain_warp(int precision, const double* d_acol, const int64_t* d_ins
                        void* stream);
 
 /*
- * One tier of a length-sorted batch: as pe_fock_chain (warp = 0) or pe_fock_chain_warp (warp = 1), but the
+ * One tier of a length-sorted batch: as pe_fock_chain (warp = 0) or pe_fock_chain_warp (warp = 1; there
+ * block_threads / 32 is the number of streams per CTA, 1 to 8, 0 = 8), but the
  * persistent queue runs only d_order[lo .. hi) with d_qrange = {lo, hi} read ON THE DEVICE (so a captured
  * CUDA graph replays it for every batch), and the kernel is chosen for chains of at most nk_max photons
  * (nk_max <= n_stride; a stream of the range with more is reported through the status word).  Launching

@@ -20,18 +20,19 @@ PE_ERR_CUDA = -3
 PE_ERR_DEVICE = -4
 PE_PRECISION_F64 = 0
 PE_PRECISION_MIXED = 1
+PE_PRECISION_COMPENSATED = 2
 PE_MAX_PHOTONS = 64
-PE_MIXED_MAX_PHOTONS = 32          # the mixed form's FP32 error grows ~1.35x per column: FP64 beyond 32
+PE_MIXED_MAX_PHOTONS = 32          # the FP32 forms are compiled up to 32 columns: FP64 beyond
 
 
 def check_photons(n: int, precision: str, what: str = "photons per stream") -> None:
     """ValueError unless the library runs chains of n photons in this precision."""
     if n > PE_MAX_PHOTONS:
         raise ValueError(f"at most {PE_MAX_PHOTONS} {what} (got {n})")
-    if precision == "mixed" and n > PE_MIXED_MAX_PHOTONS:
-        raise ValueError(f"precision='mixed' runs at most {PE_MIXED_MAX_PHOTONS} {what} (got {n}); "
+    if precision in ("mixed", "compensated") and n > PE_MIXED_MAX_PHOTONS:
+        raise ValueError(f"precision={precision!r} runs at most {PE_MIXED_MAX_PHOTONS} {what} (got {n}); "
                          f"use precision='f64'")
-PRECISIONS = {"f64": PE_PRECISION_F64, "mixed": PE_PRECISION_MIXED}
+PRECISIONS = {"f64": PE_PRECISION_F64, "mixed": PE_PRECISION_MIXED, "compensated": PE_PRECISION_COMPENSATED}
 
 _lib = None
 _vp = ctypes.c_void_p

@@ -1,6 +1,8 @@
 """Launch-shape autotuner for the chain kernel.
 
-Candidates are (threads per Gray lane, CTA threads).  `tune` times each candidate on the caller's actual
+Candidates are (threads per Gray lane, CTA threads): the lane width and CTA of the CTA-per-stream form, and
+for the warp-per-stream form the lane width and the streams per CTA (CTA threads / 32).  The batched
+sampler also tunes its length-tier cut points through `tune` (candidates are indices into its list).  `tune` times each candidate on the caller's actual
 workload (a callable running one launch with that shape), keeps the fastest, and caches the choice in a
 JSON file keyed by the GPU name, the precision and a workload key, so later processes reuse it.  The cache
 lives at $PE_TUNE_CACHE (default ~/.cache/photonic_engines_b200/tune.json).
@@ -12,7 +14,8 @@ import os
 
 import torch
 
-WARP_CANDIDATES = [(1, 256), (2, 256)]          # the warp form: threads per lane; the CTA is 8 warps
+# the warp form: (threads per lane, CTA threads = 32 x streams per CTA)
+WARP_CANDIDATES = [(1, 256), (2, 256), (1, 128), (2, 128), (1, 64)]
 CANDIDATES = {8: [(1, 128), (1, 256), (2, 128), (2, 256)],
               16: [(1, 128), (2, 128), (2, 256), (4, 256)],
               20: [(1, 128), (2, 128), (2, 256), (4, 128), (4, 256)],
@@ -21,6 +24,9 @@ CANDIDATES = {8: [(1, 128), (1, 256), (2, 128), (2, 256)],
               32: [(2, 64), (2, 128), (4, 128), (4, 256)],
               40: [(2, 64), (2, 128), (4, 128)], 48: [(4, 64), (4, 128)], 56: [(4, 64), (4, 128)],
               64: [(4, 64), (4, 128)]}
+# the compensated form is compiled for one-thread lanes at 8 columns, two-thread lanes to 20, four beyond
+COMP_CANDIDATES = {8: [(1, 128), (2, 128)], 16: [(2, 128)], 20: [(2, 128)], 24: [(4, 128)], 28: [(4, 128)],
+                   32: [(4, 128)]}
 
 
 def _cache_path() -> str:
@@ -57,7 +63,7 @@ def tier(n: int) -> int:
 
 # bumped whenever the compiled launch shapes change, so that a cached choice the library no longer accepts
 # is never replayed
-SHAPES_VERSION = 3
+SHAPES_VERSION = 4
 
 
 def key(device, precision: str, workload: str) -> str:
@@ -77,7 +83,9 @@ def tune(run, device, precision: str, n_tier: int, workload: str, reps: int = 2,
     if not force and k in cache:
         return tuple(cache[k])
     best, best_ms = None, float("inf")
-    for tpl, block in (candidates or CANDIDATES[n_tier]):
+    if candidates is None:
+        candidates = (COMP_CANDIDATES if precision == "compensated" else CANDIDATES)[n_tier]
+    for tpl, block in candidates:
         run(tpl, block)                                         # warm-up (module load, attribute set-up)
         times = []
         for _ in range(reps):

@@ -23,10 +23,13 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include"), "-I", CSRC,
          *os.environ.get("PE_NVCC_FLAGS", "").split()]
 
-# (mixed, threads per lane, largest tier) of every compiled chain/cofactor kernel pair
+# (precision 0 FP64 / 1 mixed / 2 compensated, threads per lane, largest tier) of every compiled chain/cofactor kernel pair
 VARIANTS = [(mx, tpl, kpm) for mx in (0, 1) for tpl, kpms in ((1, (8, 16, 20)), (2, (8, 16, 20, 24, 28, 32)),
                                                               (4, (8, 16, 20, 24, 28, 32))) for kpm in kpms]
 VARIANTS += [(0, 2, 40)] + [(0, 4, kpm) for kpm in (40, 48, 56, 64)]      # beyond 32 photons: FP64 only
+# compensated mixed form (double-float state: 12 FP32 pairs per column pair): two-thread lanes up to 20
+# columns, four-thread lanes beyond
+VARIANTS += [(2, 1, 8)] + [(2, 2, kpm) for kpm in (8, 16, 20)] + [(2, 4, kpm) for kpm in (24, 28, 32)]
 if os.environ.get("PE_VARIANTS"):          # a subset "m,t,k;m,t,k" (experiments: smaller, faster builds)
     VARIANTS = [tuple(int(x) for x in v.split(",")) for v in os.environ["PE_VARIANTS"].split(";")]
 
@@ -36,8 +39,12 @@ def variant_flags(mx: int, tpl: int, kpm: int) -> list[str]:
     24 to 40, four-thread lanes of 40 to 64) are compiled for 128-thread CTAs, two per SM, so that every
     thread may use 255 registers;
     the others for 256-thread CTAs at 128 registers.  Two-thread lanes at 24-32 columns compiled this way
-    run 1.1-1.9x faster than four-thread lanes at 128 registers (FP64, m = 2n)."""
+    run 1.1-1.9x faster than four-thread lanes at 128 registers (FP64, m = 2n).  The compensated form keeps
+    a double-float column sum, accumulator and prefix product per column: its two-thread lanes from 16
+    columns and four-thread lanes from 24 get the 255-register allocation too."""
     if (tpl == 1 and kpm >= 16) or (tpl == 2 and kpm >= 24) or (tpl == 4 and kpm > 32):
+        return ["-DPE_MAXT=128", "-DPE_MINB=2"]
+    if mx == 2 and ((tpl == 2 and kpm >= 16) or (tpl == 4 and kpm >= 24)):
         return ["-DPE_MAXT=128", "-DPE_MINB=2"]
     return []
 

@@ -21,6 +21,10 @@ from .. import _native as N
 from .. import autotune
 from .kernels import WARP_MAX_PHOTONS, default_tpl, pack_ragged, split_plan, use_warp_form
 
+DEFAULT_CUTS = (20, 16)
+# tier cut points the autotuner tries (descending; the last tier <= 16 photons runs in the warp form)
+CUT_CANDIDATES = [(20, 16), (24, 16), (20, 12), (24, 20, 16), (16,), (20, 16, 12)]
+
 
 def _per_instance(v, G, default):
     if v is None:
@@ -37,7 +41,7 @@ class BatchedSampler:
 
     circuits: [(U_g [m_g, m_g] complex CUDA tensor, in_modes_g)], shots: int or per-circuit list,
     loss: transmission eta (scalar or per circuit), indist: x-model overlap x (scalar or per circuit),
-    precision: "f64" | "mixed", seed: seeds the device generator, graph: capture the batch in a CUDA graph,
+    precision: "f64" | "mixed" | "compensated", seed: seeds the device generator, graph: capture the batch in a CUDA graph,
     tune: pick the launch shape with the autotuner (cached per GPU and workload); tiers: run chains of
     different lengths in kernels sized to them (False: one launch sized to the longest).
     """
@@ -47,7 +51,7 @@ class BatchedSampler:
         if not circuits:
             raise ValueError("at least one circuit")
         if precision not in N.PRECISIONS:
-            raise ValueError(f"unknown precision {precision!r}: 'f64' or 'mixed'")
+            raise ValueError(f"unknown precision {precision!r}: 'f64', 'mixed' or 'compensated'")
         U0 = circuits[0][0]
         N.require_cuda(U0, "U")
         self.device = U0.device
@@ -93,7 +97,8 @@ class BatchedSampler:
         self.rows = torch.zeros(C, ns, dtype=torch.int64, device=dev)
         self.occ = torch.zeros(S, self.m_max, dtype=torch.int64, device=dev)
         self.status = torch.zeros(2, dtype=torch.int32, device=dev)
-        self.warp = use_warp_form(self.S, self.n_stride, dev)           # short chains: one warp per stream
+        # short chains: one warp per stream (FP64 and mixed forms; the compensated form runs CTAs only)
+        self.warp = precision != "compensated" and use_warp_form(self.S, self.n_stride, dev)
         self.split = None if self.warp else split_plan(self.S, self.n_stride, dev, 0,           # few long chains
                                                         default_tpl(self.n_stride, precision), precision)
         if self.split:
@@ -103,28 +108,45 @@ class BatchedSampler:
             self.ws = N.workspace(dev)
         # length tiers: when the chains of a batch differ in length (loss, singles, circuits of several n),
         # every chain runs in the smallest kernel that holds it — the length-sorted order is cut on the device
-        # into > 20, 17..20 and <= 16 photons (the last in the warp form), one launch per tier on its own
-        # stream with its own workspace (pe_fock_chain_range), so the graph replays the cut for every batch
+        # at the tier cut points (default > 20, 17..20 and <= 16 photons, the last in the warp form), one
+        # launch per tier on its own stream with its own workspace (pe_fock_chain_range), so the graph
+        # replays the cut for every batch; the autotuner may pick other cut points
         varied = self.singles or any(e < 1.0 for e in etas) or len(set(self.n)) > 1
-        self.tiers = []
-        if tiers and varied and not self.warp and not self.split and self.n_stride > WARP_MAX_PHOTONS:
-            self.tiers = [(self.n_stride, 0)] + ([(20, 0)] if self.n_stride > 20 else []) + [(WARP_MAX_PHOTONS, 1)]
-            self.tier_thr = torch.tensor([t[0] for t in self.tiers[1:]], dtype=torch.int32, device=dev)
-            self.qr = torch.zeros(len(self.tiers), 2, dtype=torch.int64, device=dev)
-            self.qr[-1, 1] = C                                           # the cuts between tiers move per batch
-            wsb = int(N.load().pe_chain_workspace_bytes(C))
-            self.tier_ws = [torch.zeros(wsb, dtype=torch.uint8, device=dev) for _ in self.tiers]
-            self.tier_streams = [torch.cuda.Stream(dev) for _ in self.tiers[1:]]
+        self.tiered = bool(tiers and varied and not self.warp and not self.split and self.n_stride > WARP_MAX_PHOTONS)
+        self.wsb = int(N.load().pe_chain_workspace_bytes(C))
+        self.qr_all = torch.tensor([0, C], dtype=torch.int64, device=dev)      # the whole queue (warp form)
+        self._set_tiers(DEFAULT_CUTS if self.tiered else ())
         self.gen = torch.Generator(device=dev).manual_seed(seed)
         self._row0 = [0]
         for s_ in shots_l:
             self._row0.append(self._row0[-1] + s_)
         self.tpl, self.block = tpl, block_threads
+        self.warp_block = 0                                          # streams per CTA of a warp-form tier x 32
+        if tune and self.tiered:
+            self._tune_cuts()
         if tune and not (tpl and block_threads):
             self._autotune()
         self.graph = None
         if graph:
             self._capture()
+
+    def _set_tiers(self, cuts):
+        """Tiers for cut points `cuts` (descending photon counts): chains above cuts[0] in the batch's own
+        kernel, then one tier per interval, the last (<= cuts[-1], at most 16 photons) in the warp form for
+        the FP64 and mixed forms.  Empty `cuts`: no tiers."""
+        dev = self.device
+        cuts = tuple(c for c in cuts if c < self.n_stride)
+        self.cuts = cuts
+        self.tiers = []
+        if not cuts:
+            return
+        last_warp = 1 if (cuts[-1] <= WARP_MAX_PHOTONS and self.precision != "compensated") else 0
+        self.tiers = [(self.n_stride, 0)] + [(c, 0) for c in cuts[:-1]] + [(cuts[-1], last_warp)]
+        self.tier_thr = torch.tensor([t[0] for t in self.tiers[1:]], dtype=torch.int32, device=dev)
+        self.qr = torch.zeros(len(self.tiers), 2, dtype=torch.int64, device=dev)
+        self.qr[-1, 1] = self.C                                      # the cuts between tiers move per batch
+        self.tier_ws = [torch.zeros(self.wsb, dtype=torch.uint8, device=dev) for _ in self.tiers]
+        self.tier_streams = [torch.cuda.Stream(dev) for _ in self.tiers[1:]]
 
     # ---------------------------------------------------------------------------------------- one batch
     def _draw_keys(self):
@@ -160,14 +182,17 @@ class BatchedSampler:
             for i, (nk_max, warp) in enumerate(self.tiers):
                 stream = cur if i == 0 else self.tier_streams[i - 1]
                 b, t = (block, tpl) if i == 0 else (0, 0)          # the tuned shape is the top tier's
+                if warp:
+                    b, t = self.warp_block, 0
                 rc = L.pe_fock_chain_range(*common, N.ptr(self.tier_ws[i]), self.tier_ws[i].numel(), b, t, 0,
                                            N.ptr(self.qr[i]), nk_max, warp, stream.cuda_stream)
                 N.check(rc, "pe_fock_chain_range")
             for s_ in self.tier_streams:
                 cur.wait_stream(s_)
             return
-        if self.warp:
-            rc = L.pe_fock_chain_warp(*common, N.ptr(self.ws), self.ws.numel(), tpl if tpl in (1, 2) else 0, 0, st)
+        if self.warp:                  # the whole queue in the warp form, block / 32 streams per CTA
+            rc = L.pe_fock_chain_range(*common, N.ptr(self.ws), self.ws.numel(), block, tpl if tpl in (1, 2) else 0,
+                                       0, N.ptr(self.qr_all), self.n_stride, 1, st)
         elif self.split:
             rc = L.pe_fock_chain_split(*common, self.split[0], self.split[1], N.ptr(self.ws), self.ws.numel(), block,
                                        tpl, st)
@@ -187,14 +212,40 @@ class BatchedSampler:
         self._chains()
         self._scatter()
 
+    def _tune_cuts(self):
+        """Pick the tier cut points: every candidate set is timed on this batch (partition drawn once), the
+        fastest kept and cached per GPU and workload like the launch shape."""
+        workload = (f"cuts|G{self.G}|S{self.S}|m{self.m_max}|n{self.n_stride}|singles{int(self.singles)}|"
+                    f"{self.precision}")
+        cands = [c for c in CUT_CANDIDATES if all(x < self.n_stride for x in c)] or [DEFAULT_CUTS]
+        self._draw_keys()
+        self._partition()
+
+        def run(i, _block):
+            self._set_tiers(cands[i])
+            self._chains()
+        best = autotune.tune(run, self.device, self.precision, 0, workload,
+                             candidates=[(i, 0) for i in range(len(cands))])
+        self._set_tiers(cands[best[0]])
+
     def _autotune(self):
         workload = (f"batch|G{self.G}|S{self.S}|m{self.m_max}|n{self.n_stride}|singles{int(self.singles)}|"
                     f"{'warp' if self.warp else 'cta'}|tiers{len(self.tiers)}")
         self._draw_keys()
         self._partition()
-        best = autotune.tune(lambda tpl, block: self._chains(tpl, block), self.device, self.precision,
-                             autotune.tier(self.n_stride), workload,
-                             candidates=autotune.WARP_CANDIDATES if self.warp else None)
+        if self.warp:
+            best = autotune.tune(lambda tpl, block: self._chains(tpl, block), self.device, self.precision,
+                                 autotune.tier(self.n_stride), workload, candidates=autotune.WARP_CANDIDATES)
+        else:
+            best = autotune.tune(lambda tpl, block: self._chains(tpl, block), self.device, self.precision,
+                                 autotune.tier(self.n_stride), workload + f"|cuts{self.cuts}")
+            if self.tiers and self.tiers[-1][1]:                     # streams per CTA of the warp-form tier
+                def run_warp(_tpl, block):
+                    self.warp_block = block
+                    self._chains()
+                wb = autotune.tune(run_warp, self.device, self.precision, 16, workload + f"|cuts{self.cuts}|warptier",
+                                   candidates=[(0, b) for b in (64, 128, 256)])
+                self.warp_block = wb[1]
         self.tpl, self.block = best
 
     def _capture(self):

@@ -73,8 +73,10 @@ DEFAULT_BLOCK = 128          # the library's CTA size when the caller passes 0 (
 def default_tpl(n: int, precision: str) -> int:
     """Threads per Gray lane the library picks when the caller passes 0 (fock_api.cu default_tpl)."""
     kpm = next((k for k in (8, 16, 20, 24, 28, 32, 40, 48, 56, 64) if n <= k), 64)
-    if kpm <= 8 or (precision == "f64" and kpm == 20):
+    if kpm <= 8 or (precision != "compensated" and kpm == 20):
         return 1
+    if precision == "compensated":
+        return 2 if kpm <= 20 else 4
     return 2 if kpm <= 40 else 4
 
 
@@ -157,7 +159,7 @@ def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst
     dev = acol.device
     L = N.load()
     if precision not in N.PRECISIONS:
-        raise ValueError(f"unknown precision {precision!r}: 'f64' or 'mixed'")
+        raise ValueError(f"unknown precision {precision!r}: 'f64', 'mixed' or 'compensated'")
     dp = _i64(dp, dev)
     cols = _i64(cols, dev)
     S, n_stride = cols.shape
@@ -191,7 +193,8 @@ def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst
               int(occ_stride), N.ptr(marg), int(m_max))
     if mode not in ("auto", "cta", "warp"):
         raise ValueError(f"unknown mode {mode!r}: 'auto', 'cta' or 'warp'")
-    warp = (mode == "warp") or (mode == "auto" and not split and use_warp_form(S, n_stride, dev))
+    warp = (mode == "warp") or (mode == "auto" and not split and precision != "compensated"
+                                and use_warp_form(S, n_stride, dev))
     if warp:
         ws = N.workspace(dev)
         rc = L.pe_fock_chain_warp(*common, N.ptr(ws), int(ws.numel()), int(tpl if tpl in (1, 2) else 0),
@@ -226,7 +229,7 @@ def chain_adaptive(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Ten
     dev = acol.device
     L = N.load()
     if precision not in N.PRECISIONS:
-        raise ValueError(f"unknown precision {precision!r}: 'f64' or 'mixed'")
+        raise ValueError(f"unknown precision {precision!r}: 'f64', 'mixed' or 'compensated'")
     dp = _i64(dp, dev)
     cols = _i64(cols, dev)
     S, n = cols.shape
@@ -250,7 +253,8 @@ def chain_adaptive(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Ten
     occ = torch.zeros(S, m_max, dtype=torch.int64, device=dev)
     if mode not in ("auto", "cta", "warp"):
         raise ValueError(f"unknown mode {mode!r}: 'auto', 'cta' or 'warp'")
-    warp = (mode == "warp") or (mode == "auto" and not split and use_warp_form(S, n, dev))
+    warp = (mode == "warp") or (mode == "auto" and not split and precision != "compensated"
+                                and use_warp_form(S, n, dev))
     k_split, nch = (0, 0) if (warp or not split) else split
     ws = torch.empty(int(L.pe_adaptive_workspace_bytes(S, nch)), dtype=torch.uint8, device=dev)
     a = acol if acol.dtype == torch.float64 else torch.view_as_real(acol.contiguous())

@@ -24,16 +24,18 @@ static int kpm_index(int kpm) {
     return -1;
 }
 
-static void* g_chain[2][3][N_KPM];
-static void* g_cof[2][3][N_KPM];
-static void* g_split_partial[2][3][N_KPM];
-static void* g_split_draw[2][3][N_KPM];
-static void* g_warp[2][3][N_KPM];
+constexpr int N_PREC = 3;       // PE_PRECISION_F64, _MIXED, _COMPENSATED
+static void* g_chain[N_PREC][3][N_KPM];
+static void* g_cof[N_PREC][3][N_KPM];
+static void* g_split_partial[N_PREC][3][N_KPM];
+static void* g_split_draw[N_PREC][3][N_KPM];
+static void* g_warp[N_PREC][3][N_KPM];
+static bool prec_ok(int p) { return p >= 0 && p < N_PREC; }
 
 void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cofactor_kernel, void* split_partial,
                       void* split_draw, void* warp_kernel) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
-    if (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) return;
+    if (!prec_ok(mixed) || ti < 0 || ki < 0) return;
     g_warp[mixed][ti][ki] = warp_kernel;
     g_chain[mixed][ti][ki] = chain_kernel;
     g_cof[mixed][ti][ki] = cofactor_kernel;
@@ -42,33 +44,35 @@ void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cof
 }
 void* find_split_partial_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
-    return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_split_partial[mixed][ti][ki];
+    return (!prec_ok(mixed) || ti < 0 || ki < 0) ? nullptr : g_split_partial[mixed][ti][ki];
 }
 void* find_warp_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
-    return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_warp[mixed][ti][ki];
+    return (!prec_ok(mixed) || ti < 0 || ki < 0) ? nullptr : g_warp[mixed][ti][ki];
 }
-size_t warp_smem_bytes() { return sizeof(WarpSmem) * WARPS; }
+size_t warp_smem_bytes(int warps) { return sizeof(WarpSmem) * (size_t)warps; }
 void* find_split_draw_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
-    return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_split_draw[mixed][ti][ki];
+    return (!prec_ok(mixed) || ti < 0 || ki < 0) ? nullptr : g_split_draw[mixed][ti][ki];
 }
 void* find_chain_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
-    return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_chain[mixed][ti][ki];
+    return (!prec_ok(mixed) || ti < 0 || ki < 0) ? nullptr : g_chain[mixed][ti][ki];
 }
 void* find_cofactor_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
-    return (mixed < 0 || mixed > 1 || ti < 0 || ki < 0) ? nullptr : g_cof[mixed][ti][ki];
+    return (!prec_ok(mixed) || ti < 0 || ki < 0) ? nullptr : g_cof[mixed][ti][ki];
 }
 
 // Threads per Gray lane when the caller passes 0 (measured at m = 400, 2 000 streams, and at m = 2n for
-// 21-32 photons): one-thread lanes up to 8 columns, and for FP64 chains of 17-20 photons (no exchange of
-// partial products; those variants run 128-thread CTAs with 255 registers); two-thread lanes beyond
+// 21-32 photons): one-thread lanes up to 8 columns, and for FP64 and mixed chains of 17-20 photons (no
+// exchange of partial products; those variants run 128-thread CTAs with 255 registers: n = 20, m = 400,
+// FP64 18.4 against 21.0 ms with two-thread lanes, mixed 12.8 against 13.4 ms); two-thread lanes beyond
 // (at 24-40 columns compiled for 128-thread CTAs with 255 registers), four-thread lanes at 48-64.
 static int default_tpl(int kpm, int precision) {
     if (kpm <= 8) return 1;
-    if (precision == PE_PRECISION_F64 && kpm == 20) return 1;
+    if (precision != PE_PRECISION_COMPENSATED && kpm == 20) return 1;
+    if (precision == PE_PRECISION_COMPENSATED) return kpm <= 20 ? 2 : 4;   // 12 FP32 pairs of state per column pair
     return kpm <= 40 ? 2 : 4;
 }
 
@@ -254,7 +258,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
                         int grid_ctas, int k_split, int nch, void* stream, bool warp_mode = false,
                         int k_first = 1, int k_last = 0, bool zero_status = true,
                         const int64_t* d_qrange = nullptr, int nk_max = 0) {
-    if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
+    if (!prec_ok(precision)) return PE_ERR_ARG;
     if (nk_max < 0 || nk_max > n_stride || (d_qrange && k_split > 0)) return PE_ERR_ARG;
     if (k_first < 1 || k_first > n_stride + 1 || k_last < 0) return PE_ERR_ARG;
     if (S < 0 || G < 1 || m_max < 1 || n_stride < 1) return PE_ERR_ARG;
@@ -271,7 +275,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     const int kpm = kpm_for(ncols);
     if (kpm < 0) return PE_ERR_SIZE;
     if (kpm > NARROW && precision != PE_PRECISION_F64) return PE_ERR_SIZE;   // mixed form: up to 32 columns
-    if (warp_mode && (kpm > WMAXN || split)) return PE_ERR_SIZE;
+    if (warp_mode && (kpm > WMAXN || split || precision == PE_PRECISION_COMPENSATED)) return PE_ERR_SIZE;
     if (tpl == 0) {
         tpl = warp_mode ? (kpm <= 8 ? 1 : 2) : default_tpl(kpm, precision);
         if (!warp_mode && !find_chain_kernel(precision, tpl, kpm)) tpl = find_chain_kernel(precision, 2, kpm) ? 2 : 4;
@@ -283,9 +287,13 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     if (bmax < 32) return PE_ERR_CUDA;
     // default CTA: 128 threads (as many warps per SM as 256-thread CTAs, twice the CTAs to overlap the
     // per-step serial phases of one stream with the sweeps of others)
-    const int block = warp_mode ? 32 * WARPS : (block_threads ? block_threads : (bmax < 128 ? bmax : 128));
-    if (block < 32 || block > 256 || block > bmax || (block & 31) || block < ncols) return PE_ERR_ARG;
-    const size_t smem = warp_mode ? warp_smem_bytes() : smem_fixed_bytes_for(kpm) + (size_t)m_max * sizeof(double);
+    // warp form: one stream per warp, block_threads / 32 streams per CTA (default 8)
+    const int block = warp_mode ? (block_threads ? block_threads : 32 * WARPS)
+                                : (block_threads ? block_threads : (bmax < 128 ? bmax : 128));
+    if (block < 32 || block > 256 || block > bmax || (block & 31)) return PE_ERR_ARG;
+    if (!warp_mode && block < ncols) return PE_ERR_ARG;
+    const size_t smem_fix = smem_fixed_bytes_for(kpm, precision);
+    const size_t smem = warp_mode ? warp_smem_bytes(block / 32) : smem_fix + (size_t)m_max * sizeof(double);
     const int cap = max_smem_optin();
     if (cap <= 0) return PE_ERR_CUDA;
     if (smem > (size_t)cap) return PE_ERR_SIZE;
@@ -300,7 +308,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int64_t grid = grid_ctas > 0 ? grid_ctas : (int64_t)sms * per_sm;
-    const int64_t units = warp_mode ? (S + WARPS - 1) / WARPS : S;      // streams in flight per CTA
+    const int64_t units = warp_mode ? (S + block / 32 - 1) / (block / 32) : S;   // streams in flight per CTA
     if (grid > units) grid = units;
     if (grid < 1) grid = 1;
     ChainParams p;
@@ -314,14 +322,20 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     p.status = (int*)((char*)d_workspace + 8);
     p.detail = (long long*)((char*)d_workspace + 16);
     p.m_cap = m_max;
-    p.tau = 1.0e-5;            // mixed guard band: 3x the largest measured CDF deviation (3.3e-6, n <= 28)
+    // Guard bands of the mixed forms.  Mixed: the largest CDF deviation from FP64 measured on chain rows of
+    // Haar circuits (m = 400, 784, 900; 24-64 chains, up to 32 columns) is 1.1e-6 at 20 columns and grows
+    // about 1.19x per column (7.8e-6 at 32); the band is 8x that envelope, about 2 tau m of the draws
+    // redo their step in FP64.  Compensated: its blocks are FP64-accurate (~1e-10); the band only keeps
+    // its picks the FP64 form's where the two round differently.
+    p.tau = precision == PE_PRECISION_COMPENSATED ? 1.0e-8 : 8.0e-6;
+    p.tau_log2g = 0.251;       // log2(1.19)
     p.k_first = k_first;
     p.k_stop = split ? (k_split - 1 < klast ? k_split - 1 : klast) : (k_last > 0 ? klast : 0);
     void* args[] = {&p};
     PE_CUDA_TRY(cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st));
     if (!split) return PE_OK;
     // the mixed form's guard band: flagged streams redo the step with the FP64 kernels (second pass)
-    const int npass = precision == PE_PRECISION_MIXED ? 2 : 1;
+    const int npass = precision != PE_PRECISION_F64 ? 2 : 1;
     void* fpart[2] = {find_split_partial_kernel(precision, tpl, kpm), find_split_partial_kernel(PE_PRECISION_F64, tpl, kpm)};
     void* fdraw[2] = {find_split_draw_kernel(precision, tpl, kpm), find_split_draw_kernel(PE_PRECISION_F64, tpl, kpm)};
     int64_t gpart[2], gdraw[2];
@@ -329,8 +343,10 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     for (int q = 0; q < npass; ++q) {
         if (!fpart[q] || !fdraw[q]) return PE_ERR_SIZE;
         int per_part = 0, per_draw = 0;
-        if ((rc = launch_prepare(fpart[q], block, smem_fixed_bytes_for(kpm), &per_part)) != PE_OK) return rc;
-        if ((rc = launch_prepare(fdraw[q], block, smem, &per_draw)) != PE_OK) return rc;
+        const int pq = q == 0 ? precision : PE_PRECISION_F64;
+        const size_t sdraw = smem_fixed_bytes_for(kpm, pq) + (size_t)m_max * sizeof(double);
+        if ((rc = launch_prepare(fpart[q], block, smem_fixed_bytes_for(kpm, pq), &per_part)) != PE_OK) return rc;
+        if ((rc = launch_prepare(fdraw[q], block, sdraw, &per_draw)) != PE_OK) return rc;
         gpart[q] = items < (int64_t)sms * per_part ? items : (int64_t)sms * per_part;
         gdraw[q] = S < (int64_t)sms * per_draw ? S : (int64_t)sms * per_draw;
     }
@@ -344,9 +360,11 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
         sp.k = k;
         for (int q = 0; q < npass; ++q) {
             sp.pass = q;
-            PE_CUDA_TRY(cudaLaunchKernel(fpart[q], dim3((unsigned)gpart[q]), dim3(block), sargs, smem_fixed_bytes_for(kpm),
-                                         st));
-            PE_CUDA_TRY(cudaLaunchKernel(fdraw[q], dim3((unsigned)gdraw[q]), dim3(block), sargs, smem, st));
+            const int pq = q == 0 ? precision : PE_PRECISION_F64;
+            PE_CUDA_TRY(cudaLaunchKernel(fpart[q], dim3((unsigned)gpart[q]), dim3(block), sargs,
+                                         smem_fixed_bytes_for(kpm, pq), st));
+            PE_CUDA_TRY(cudaLaunchKernel(fdraw[q], dim3((unsigned)gdraw[q]), dim3(block), sargs,
+                                         smem_fixed_bytes_for(kpm, pq) + (size_t)m_max * sizeof(double), st));
         }
     }
     return PE_OK;
@@ -375,7 +393,7 @@ extern "C" int pe_fock_chain_range(int precision, const double* d_acol, const in
     if (!d_qrange || !d_order || !d_nk || nk_max < 1 || (warp != 0 && warp != 1)) return PE_ERR_ARG;
     return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, d_nk, d_cols, n_stride,
                         d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ, occ_stride, d_marg,
-                        marg_stride, d_workspace, workspace_bytes, warp ? 0 : block_threads, tpl, grid_ctas, 0, 1,
+                        marg_stride, d_workspace, workspace_bytes, block_threads, tpl, grid_ctas, 0, 1,
                         stream, warp == 1, 1, 0, true, d_qrange, nk_max);
 }
 
@@ -472,14 +490,14 @@ extern "C" int pe_fock_chain_adaptive(int precision, const double* d_acol, const
 extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t* d_rows, int64_t S, int m, int K,
                                  double* d_p, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
                                  void* stream) {
-    if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
+    if (!prec_ok(precision)) return PE_ERR_ARG;
     if (S < 0 || m < 1 || K < 1 || !d_a || !d_p || !d_workspace) return PE_ERR_ARG;
     if (K > 1 && !d_rows) return PE_ERR_ARG;
     if (workspace_bytes < WS_BYTES || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
     const int kpm = kpm_for(K);
     if (kpm < 0) return PE_ERR_SIZE;
     if (kpm > NARROW && precision != PE_PRECISION_F64) return PE_ERR_SIZE;
-    if (tpl == 0) tpl = kpm <= 8 ? 1 : (kpm <= 40 ? 2 : 4);
+    if (tpl == 0) tpl = precision == PE_PRECISION_COMPENSATED ? default_tpl(kpm, precision) : (kpm <= 8 ? 1 : (kpm <= 40 ? 2 : 4));
     if (tpl_index(tpl) < 0) return PE_ERR_ARG;
     void* fn = find_cofactor_kernel(precision, tpl, kpm);
     if (!fn) return PE_ERR_SIZE;
@@ -490,7 +508,7 @@ extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t
     cudaStream_t st = (cudaStream_t)stream;
     PE_CUDA_TRY(cudaMemsetAsync(d_workspace, 0, WS_BYTES, st));
     if (S == 0) return PE_OK;
-    const size_t smem = smem_fixed_bytes_for(kpm);
+    const size_t smem = smem_fixed_bytes_for(kpm, precision);
     int per_sm = 0;
     int rc = launch_prepare(fn, block, smem, &per_sm);
     if (rc != PE_OK) return rc;
@@ -509,7 +527,7 @@ extern "C" int pe_cofactors_rows(int precision, const double* d_a, const int64_t
 }
 
 extern "C" int pe_split_slots(int precision, int n_stride, int block_threads, int tpl) {
-    if (precision != PE_PRECISION_F64 && precision != PE_PRECISION_MIXED) return PE_ERR_ARG;
+    if (!prec_ok(precision)) return PE_ERR_ARG;
     const int kpm = kpm_for(n_stride);
     if (n_stride < 1 || kpm < 0) return PE_ERR_SIZE;
     if (kpm > NARROW && precision != PE_PRECISION_F64) return PE_ERR_SIZE;
@@ -525,7 +543,7 @@ extern "C" int pe_split_slots(int precision, int n_stride, int block_threads, in
     const int block = block_threads ? block_threads : (bmax < 128 ? bmax : 128);
     if (block < 32 || block > 256 || block > bmax || (block & 31)) return PE_ERR_ARG;
     int per_sm = 0, dev = 0, sms = 0;
-    const int rc = launch_prepare(fn, block, smem_fixed_bytes_for(kpm), &per_sm);
+    const int rc = launch_prepare(fn, block, smem_fixed_bytes_for(kpm, precision), &per_sm);
     if (rc != PE_OK) return rc;
     PE_CUDA_TRY(cudaGetDevice(&dev));
     PE_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -564,6 +582,7 @@ extern "C" int pe_pipe_probe(int precision, int iters, void* d_out, size_t out_b
 // that must start at zero (queue counter, status word) on its stream before launching, and calls whose
 // kernels overlap on the GPU (different streams, or different host threads on one device) race on it.
 constexpr size_t PE_NOALLOC_SCRATCH_BYTES = 4096;
+static_assert(WS_BYTES <= PE_NOALLOC_SCRATCH_BYTES, "the chain workspace must fit the static scratch");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[PE_NOALLOC_SCRATCH_BYTES];
 
 constexpr int PE_NOALLOC_MAX_DEVICES = 64;

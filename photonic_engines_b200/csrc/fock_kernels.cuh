@@ -75,7 +75,8 @@ struct ChainParams {
     int* status;
     long long* detail;
     int m_cap;
-    double tau;     // mixed form: relative guard band of the draw
+    double tau;     // mixed forms: relative guard band of the draw at a step of 20 columns ...
+    double tau_log2g;  // ... growing by 2^tau_log2g per column (guard_band)
     int k_stop;     // run steps up to min(nk, k_stop) only (0: all); later steps go to the split kernels
     int k_first;    // first step to run (1: the whole chain); rows[s][0 .. k_first - 2] are given (a forced
                     // prefix, or the steps of an earlier launch).  A stream with nk < k_first - 1 is skipped.
@@ -91,6 +92,13 @@ constexpr int MIXED_LIN = PE_MIXED_LIN;
 constexpr size_t WS_BYTES = 256;
 
 static __device__ __forceinline__ void record_error(int* status, long long* detail, int64_t s);
+
+// Guard band of a mixed form's draw at a step of k columns, relative to the total weight: a draw whose
+// uniform lies closer than this to a CDF step is redone in FP64.  The FP32 sweeps' CDF deviation from
+// FP64 grows geometrically with k, so the band does too.
+static __device__ __forceinline__ double guard_band(const ChainParams& p, int k) {
+    return p.tau * exp2((double)(k - 20) * p.tau_log2g);
+}
 
 // The stream that queue ticket q stands for: order[lo + q] over the range [lo, hi) of the queue (qrange,
 // or the whole [0, S)); -1 once the range is drained.  An invalid range counts as empty and is recorded
@@ -951,18 +959,32 @@ __device__ void dispatch_mixed(SM& sm, int K) {
     PE_TIER(28, (sweep_mixed<28, TPL>(sm)))
     PE_TIER(32, (sweep_mixed<32, TPL>(sm)))
 }
+}  // namespace pe
 
-// One cofactor step of the stream held in shared memory (K1 >= 1): plan, prepare, sweep.
-template <int TPL, int KPM, bool MIXED, class SM>
+#include "fock_comp.cuh"
+
+namespace pe {
+
+// One cofactor step of the stream held in shared memory (K1 >= 1): plan, prepare, sweep.  PREC: 0 FP64,
+// 1 mixed, 2 compensated mixed.
+template <int TPL, int KPM, int PREC, class SM>
 __device__ __forceinline__ void cofactor_step(SM& sm, const double2* A, int64_t rs, int64_t cs, int K1, int K) {
+    constexpr bool MIXED = PREC == PREC_MIXED;
     if (threadIdx.x < 32) plan_step(sm, K1, K, blockDim.x / TPL * sm.lane_mult, MIXED ? MIXED_LIN : LIN_MAX, MID_MAX);
     __syncthreads();
     // paired FP32 sweeps (mixed form, 1- and 2-thread lanes): columns per thread of the dispatched tier
     const int kh = (MIXED && PE_PAIR32 && TPL <= 2) ? ((K + 3) / 4 * 4) / TPL : 0;
     prepare_step(sm, A, rs, cs, MIXED, kh);
     __syncthreads();
-    if constexpr (MIXED) dispatch_mixed<TPL, KPM>(sm, K);
-    else dispatch_f64<TPL, KPM>(sm, K);
+    if constexpr (PREC == PREC_COMP) {
+        prepare_comp(sm, ((K + 3) / 4 * 4) / TPL, TPL);
+        __syncthreads();
+        dispatch_comp<TPL, KPM>(sm, K);
+    } else if constexpr (MIXED) {
+        dispatch_mixed<TPL, KPM>(sm, K);
+    } else {
+        dispatch_f64<TPL, KPM>(sm, K);
+    }
 }
 
 // ---------------------------------------------------------------------------------------- draw
@@ -1062,8 +1084,8 @@ static __device__ void draw_step(SM& sm, double* __restrict__ wgt, const double2
 }
 
 // ---------------------------------------------------------------------------------------- chain
-template <int TPL, int KPM, bool MIXED>
-__device__ void chain_one(const ChainParams& p, SmemFor<KPM>& sm, double* wgt, int64_t s) {
+template <int TPL, int KPM, int PREC>
+__device__ void chain_one(const ChainParams& p, SmemFor<KPM, PREC>& sm, double* wgt, int64_t s) {
     const int tid = threadIdx.x;
     const int64_t g = p.dp[s];
     bool ok = g >= 0 && g < p.G;
@@ -1103,7 +1125,7 @@ __device__ void chain_one(const ChainParams& p, SmemFor<KPM>& sm, double* wgt, i
             if (tid == 0) sm.P[0] = make_double2(1.0, 0.0);
             __syncthreads();
         } else {
-            cofactor_step<TPL, KPM, MIXED>(sm, A, 1, m, K1, K);
+            cofactor_step<TPL, KPM, PREC>(sm, A, 1, m, K1, K);
         }
         double u;
         if (p.uniforms) {
@@ -1114,9 +1136,9 @@ __device__ void chain_one(const ChainParams& p, SmemFor<KPM>& sm, double* wgt, i
             u = chain_uniform((uint64_t)p.seeds[row * p.n_stride + (k - 1)], ro);
         }
         double* mrow = p.marg ? p.marg + ((size_t)s * p.n_stride + (k - 1)) * p.marg_stride : nullptr;
-        if constexpr (MIXED) {
+        if constexpr (PREC != PREC_F64) {
             draw_step(sm, wgt, A, 1, m, m, k, u, mrow, false);
-            if (K1 > 0 && sm.fmin[0] <= p.tau) {          // uniform: read after the draw's final barrier
+            if (K1 > 0 && sm.fmin[0] <= guard_band(p, k)) {   // uniform: read after the draw's final barrier
                 dispatch_f64<4, KPM>(sm, K);
                 draw_step(sm, wgt, A, 1, m, m, k, u, mrow, false);
             }
@@ -1137,12 +1159,12 @@ __device__ void chain_one(const ChainParams& p, SmemFor<KPM>& sm, double* wgt, i
 }
 
 
-template <int TPL, int KPM, bool MIXED>
+template <int TPL, int KPM, int PREC>
 __global__ void __launch_bounds__(PE_MAXT, PE_MINB) fock_chain_kernel(ChainParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using SM = SmemFor<KPM>;
+    using SM = SmemFor<KPM, PREC>;
     SM& sm = *reinterpret_cast<SM*>(smem_raw);
-    double* wgt = reinterpret_cast<double*>(smem_raw + smem_fixed_bytes<KPM>());
+    double* wgt = reinterpret_cast<double*>(smem_raw + smem_fixed_bytes<KPM, PREC>());
     const int tid = threadIdx.x;
     for (;;) {
         if (tid == 0) {
@@ -1156,7 +1178,7 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) fock_chain_kernel(ChainParam
             if (tid == 0) record_error(p.status, p.detail, s);
             return;
         }
-        chain_one<TPL, KPM, MIXED>(p, sm, wgt, s);
+        chain_one<TPL, KPM, PREC>(p, sm, wgt, s);
         __syncthreads();
     }
 }
@@ -1171,7 +1193,7 @@ struct SplitParams {
     int k;                  // the step (k columns, k - 1 chosen rows), k >= 2
     int nch;                // CTAs per stream at this step
     double2* partial;       // [S][nch][MAXN]
-    int* flag;              // [S] mixed form: 1 when the draw fell in the guard band (redo this step in FP64)
+    int* flag;              // [S] mixed forms: 1 when the draw fell in the guard band (redo this step in FP64)
     int pass;               // 0: the step; 1: only the flagged streams (FP64 kernels)
 };
 
@@ -1212,10 +1234,10 @@ static __device__ bool load_state(const ChainParams& p, SM& sm, int64_t s, int k
     return true;
 }
 
-template <int TPL, int KPM, bool MIXED>
+template <int TPL, int KPM, int PREC>
 __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_partial_kernel(SplitParams sp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using SM = SmemFor<KPM>;
+    using SM = SmemFor<KPM, PREC>;
     SM& sm = *reinterpret_cast<SM*>(smem_raw);
     const ChainParams& p = sp.c;
     const int tid = threadIdx.x, k = sp.k;
@@ -1228,7 +1250,7 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_partial_kernel(SplitPa
         if (live) {
             if (tid == 0) { sm.lane0 = (int64_t)i * (blockDim.x / TPL); sm.lane_mult = sp.nch; }
             __syncthreads();
-            cofactor_step<TPL, KPM, MIXED>(sm, p.acol + off, 1, m, k - 1, k);
+            cofactor_step<TPL, KPM, PREC>(sm, p.acol + off, 1, m, k - 1, k);
             if (tid < k) sp.partial[(s * sp.nch + i) * MAXN + tid] = sm.P[tid];
         }
         __syncthreads();
@@ -1237,12 +1259,12 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_partial_kernel(SplitPa
 
 // TPL does not enter the draw; it keeps the kernel's symbol distinct in every variant object, whose
 // launch bounds differ (one shared symbol would let the runtime launch any object's copy).
-template <int TPL, int KPM, bool MIXED>
+template <int TPL, int KPM, int PREC>
 __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_draw_kernel(SplitParams sp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using SM = SmemFor<KPM>;
+    using SM = SmemFor<KPM, PREC>;
     SM& sm = *reinterpret_cast<SM*>(smem_raw);
-    double* wgt = reinterpret_cast<double*>(smem_raw + smem_fixed_bytes<KPM>());
+    double* wgt = reinterpret_cast<double*>(smem_raw + smem_fixed_bytes<KPM, PREC>());
     const ChainParams& p = sp.c;
     const int tid = threadIdx.x, k = sp.k;
     for (int64_t s = blockIdx.x; s < p.S; s += gridDim.x) {
@@ -1271,8 +1293,8 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_draw_kernel(SplitParam
         }
         double* mrow = p.marg ? p.marg + ((size_t)s * p.n_stride + (k - 1)) * p.marg_stride : nullptr;
         draw_step(sm, wgt, A, 1, m, m, k, u, mrow, false);
-        if constexpr (MIXED) {
-            const bool redo = sm.fmin[0] <= p.tau;       // guard band: the FP64 pass redoes this step
+        if constexpr (PREC != PREC_F64) {
+            const bool redo = sm.fmin[0] <= guard_band(p, k);   // guard band: the FP64 pass redoes this step
             if (tid == 0) sp.flag[s] = redo ? 1 : 0;
             if (redo) { __syncthreads(); continue; }
         } else {
@@ -1292,12 +1314,12 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_draw_kernel(SplitParam
 }
 
 // Cofactors of S independent blocks: A [S][m][K] row-major, rows [S][K - 1].
-template <int TPL, int KPM, bool MIXED>
+template <int TPL, int KPM, int PREC>
 __global__ void __launch_bounds__(256) cofactor_kernel(const double2* __restrict__ A, const int64_t* __restrict__ rows,
                                                        int64_t S, int m, int K, double2* __restrict__ P,
                                                        int* status, long long* detail) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    using SM = SmemFor<KPM>;
+    using SM = SmemFor<KPM, PREC>;
     SM& sm = *reinterpret_cast<SM*>(smem_raw);
     const int tid = threadIdx.x;
     for (int64_t s = blockIdx.x; s < S; s += gridDim.x) {
@@ -1321,7 +1343,7 @@ __global__ void __launch_bounds__(256) cofactor_kernel(const double2* __restrict
             if (tid == 0) sm.P[0] = make_double2(1.0, 0.0);
             __syncthreads();
         } else {
-            cofactor_step<TPL, KPM, MIXED>(sm, A + s * (int64_t)m * K, K, 1, K - 1, K);
+            cofactor_step<TPL, KPM, PREC>(sm, A + s * (int64_t)m * K, K, 1, K - 1, K);
         }
         if (tid < K) P[s * K + tid] = sm.P[tid];
         __syncthreads();

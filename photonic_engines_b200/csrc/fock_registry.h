@@ -11,6 +11,6 @@ void* find_cofactor_kernel(int mixed, int tpl, int kpm);
 void* find_split_partial_kernel(int mixed, int tpl, int kpm);
 void* find_split_draw_kernel(int mixed, int tpl, int kpm);
 void* find_warp_kernel(int mixed, int tpl, int kpm);
-size_t warp_smem_bytes();
+size_t warp_smem_bytes(int warps);
 
 }  // namespace pe

@@ -300,7 +300,7 @@ __device__ void chain_warp(const ChainParams& p, WarpSmem& sm, int64_t s) {
         double* mrow = p.marg ? p.marg + ((size_t)s * p.n_stride + (k - 1)) * p.marg_stride : nullptr;
         const double gap = draw_warp(sm, A, m, k, u, mrow);
         if constexpr (MIXED) {
-            if (K1 > 0 && gap <= p.tau) {                  // guard band: this step again in FP64
+            if (K1 > 0 && gap <= guard_band(p, k)) {       // guard band: this step again in FP64
                 warp_cofactors<TPL, KPW, false>(sm, k);
                 draw_warp(sm, A, m, k, u, mrow);
             }

@@ -86,15 +86,19 @@ struct PlanT {
 
 // Shared memory of one CTA working on one stream, for tiers of up to NK columns (32: the narrow layout
 // of chains up to 32 photons; 64: the wide one, FP64 only, so its FP32 copy of B is a placeholder).
-template <int NK>
+// COMP: the compensated form's layout, with the low parts of 2B beside the high ones.
+template <int NK, bool COMP = false>
 struct SmemT {
     static constexpr int NKMAX = NK;
     static constexpr int NK32 = NK <= NARROW ? NK : 1;
+    static constexpr int NKLO = COMP ? NK32 : 1;
     PlanT<NK> plan;
     double2 P[NK];                 // cofactors of the step (scaled)
     double2 B[NK][NK];             // B[kd][j] = A[drow_kd, col_j], padded columns zero
     alignas(16) float2 B32[NK32][NK32];   // 2 * B in float32 (the mixed form's Gray update); paired
                                    // sweeps read each row as float4 slots (see prepare_step)
+    alignas(16) float2 B32lo[NKLO][NKLO];  // compensated form: 2B - B32 (B32 then lies on the grid)
+    double grid;                   // compensated form: power-of-two grid of the column sums' high parts
     double tab_w[LIN_MAX];         // inner weight prod (-1)^v C(M, v) at inner index t
     float tab_w32[LIN_MAX];
     double tab_wm[MID_MAX];        // middle weight at middle index
@@ -116,16 +120,20 @@ struct SmemT {
     int bad;                       // set by any thread that saw an out-of-range index
 };
 
+// Precision forms (the values of PE_PRECISION_* in pe_b200.h)
+constexpr int PREC_F64 = 0, PREC_MIXED = 1, PREC_COMP = 2;
+
 using Plan = PlanT<NARROW>;
 using Smem = SmemT<NARROW>;
-template <int KPM>
-using SmemFor = SmemT<(KPM <= NARROW ? NARROW : MAXN)>;
+template <int KPM, int PREC = PREC_F64>
+using SmemFor = SmemT<(KPM <= NARROW ? NARROW : MAXN), PREC == PREC_COMP>;
 
 // Dynamic shared memory of a chain CTA before its m weights: the layout of the tier, 16-byte rounded.
-template <int KPM>
-__host__ __device__ constexpr size_t smem_fixed_bytes() { return (sizeof(SmemFor<KPM>) + 15) & ~(size_t)15; }
-__host__ __device__ constexpr size_t smem_fixed_bytes_for(int kpm) {
-    return kpm <= NARROW ? smem_fixed_bytes<NARROW>() : smem_fixed_bytes<MAXN>();
+template <int KPM, int PREC = PREC_F64>
+__host__ __device__ constexpr size_t smem_fixed_bytes() { return (sizeof(SmemFor<KPM, PREC>) + 15) & ~(size_t)15; }
+__host__ __device__ constexpr size_t smem_fixed_bytes_for(int kpm, int prec = PREC_F64) {
+    return kpm <= NARROW ? (prec == PREC_COMP ? smem_fixed_bytes<NARROW, PREC_COMP>() : smem_fixed_bytes<NARROW>())
+                         : smem_fixed_bytes<MAXN>();
 }
 
 }  // namespace pe

@@ -1,6 +1,5 @@
 """The batched sampler (many circuits, device-side loss / distinguishability partition, one persistent
 launch, CUDA-graph replay): exact law at small sizes, per-circuit layout, graph replays."""
-import itertools
 import math
 
 import numpy as np
@@ -14,41 +13,12 @@ pytestmark = pytest.mark.gpu
 DEV = "cuda"
 
 
-def _imperfect_distribution(U, in_modes, eta, x):
-    """Exact law of lossy, x-model partially distinguishable photons: every photon independently lost
-    (1 - eta), interfering (eta x) or alone (eta (1 - x)); the interfering ones follow the permanent law,
-    each lone one lands in row r with probability |U[r, col]|^2, and the occupations add."""
-    m, n = U.shape[0], len(in_modes)
-    dist: dict = {}
-    for roles in itertools.product((0, 1, 2), repeat=n):        # 0 lost, 1 alone, 2 interfering
-        p = 1.0
-        for r in roles:
-            p *= (1 - eta) if r == 0 else (eta * (1 - x) if r == 1 else eta * x)
-        if p == 0.0:
-            continue
-        inter = [in_modes[j] for j in range(n) if roles[j] == 2]
-        lone = [in_modes[j] for j in range(n) if roles[j] == 1]
-        part = O.exact_distribution(U, inter) if inter else {tuple([0] * m): 1.0}
-        for col in lone:
-            w = np.abs(U[:, col]) ** 2
-            new: dict = {}
-            for k, q in part.items():
-                for r_ in range(m):
-                    kk = list(k)
-                    kk[r_] += 1
-                    new[tuple(kk)] = new.get(tuple(kk), 0.0) + q * w[r_]
-            part = new
-        for k, q in part.items():
-            dist[k] = dist.get(k, 0.0) + p * q
-    return dist
-
-
-@pytest.mark.parametrize("precision", ["f64", "mixed"])
+@pytest.mark.parametrize("precision", ["f64", "mixed", "compensated"])
 @pytest.mark.parametrize("eta,x", [(0.7, 1.0), (1.0, 0.6), (0.8, 0.7)])
 def test_batched_law_matches_the_exact_imperfect_distribution(precision, eta, x):
     m, in_modes, shots = 4, [0, 1, 2], 40000
     U = O.haar_unitary(m, 8)
-    dist = _imperfect_distribution(U, in_modes, eta, x)
+    dist = O.imperfect_distribution(U, in_modes, eta, x)
     assert abs(sum(dist.values()) - 1) < 1e-9
     bs = BatchedSampler([(torch.tensor(U, device=DEV), in_modes)], shots, loss=eta, indist=x, precision=precision,
                         seed=5, tune=False)
@@ -99,7 +69,7 @@ def test_graph_replays_draw_fresh_samples_and_conserve_photons():
 def test_graph_and_eager_paths_agree_in_law():
     U = O.haar_unitary(5, 4)
     circ = [(torch.tensor(U, device=DEV), [0, 1])]
-    dist = _imperfect_distribution(U, [0, 1], 0.9, 0.8)
+    dist = O.imperfect_distribution(U, [0, 1], 0.9, 0.8)
     for graph in (True, False):
         bs = BatchedSampler(circ, 30000, loss=0.9, indist=0.8, seed=11, graph=graph, tune=False)
         tvd, floor = O.tvd_and_floor(dist, bs.sample().cpu().numpy())
