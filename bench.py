@@ -32,9 +32,9 @@ sys.path.insert(0, ROOT)
 
 N_PHOT, M_MODES, SHOTS, USEED = 20, 400, 2000, 1002
 # DRAM bytes (read + write) of one chain launch on this workload, from one ncu capture of each form
-# (dram__bytes_read.sum + dram__bytes_write.sum, `--profile-launch f64|mixed`); the algorithmic bytes
+# (dram__bytes_read.sum + dram__bytes_write.sum, `--profile-launch f64|mixed|compensated`); the algorithmic bytes
 # (16 m k + 16 k^2 per sample and step, 2.78 GB per launch) are served from L2 and shared memory.
-DRAM_BYTES_PER_LAUNCH = {"f64": 1.119e6 + 0.0, "mixed": 1.008e6 + 0.023e6}
+DRAM_BYTES_PER_LAUNCH = {"f64": 1.119e6 + 0.0, "mixed": 1.008e6 + 0.023e6, "compensated": 0.807e6 + 0.0}
 METRIC = "samples/s n=20 m=400: mixed-precision vs FP64 on B200, marginal err<=1e-6"
 BOUND = 1e-6                                    # the metric's marginal error bound
 FORMS = ("f64", "mixed", "compensated")         # FP64 first: the reference every other form is measured against
@@ -411,6 +411,16 @@ def _config_circuits(name: str, dev):
     raise ValueError(name)
 
 
+def hbm_peak() -> tuple[float, str]:
+    """HBM bandwidth denominator: the measured copy bandwidth of this pool's B200s when the peaks file is
+    present, else the earlier measurement on this pool."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "of measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "of fallback (6.65 TB/s)"
+
+
 def config_result(name: str, steps: int, warmup: int) -> dict:
     """One configuration run through the batched sampler (one persistent launch per batch, CUDA-graph
     replay) in every form: samples/s, roofline of the chain kernel, end to end with the occupations copied
@@ -446,18 +456,28 @@ def config_result(name: str, steps: int, warmup: int) -> dict:
         nk = bs.nk.cpu().numpy()
         rows = bs.rows.cpu().numpy()
         dpn = bs.chain_dp.cpu().numpy()
-        flops = 0.0
+        flops = nbytes = 0.0
         for g in range(bs.G):                                # work of the last batch, per circuit (m differs)
             sel = (dpn == g) & (nk > 0)
             if sel.any():
-                flops += chain_work(rows[sel], bs.m[g], nk[sel])["flops"]
+                w = chain_work(rows[sel], bs.m[g], nk[sel])
+                flops += w["flops"]
+                nbytes += w["bytes"]
         occs[precision] = bs.occ.clone()
         ach = flops / (ms * 1e-3) / 1e12
+        hbm, hbm_src = hbm_peak()
+        gbs = nbytes / (ms * 1e-3) / 1e9
         out[precision] = {"value": bs.S / (ms * 1e-3), "ms_per_step": ms, "tpl_block": [bs.tpl, bs.block],
-                          "roofline": {"bound": "fp64" if precision == "f64" else "fp32", "achieved": ach,
-                                       "peak": peak[precision], "unit": "TFLOP/s", "frac": ach / peak[precision],
+                          "tier_cuts": list(bs.cuts), "warp_tier_block": bs.warp_block, "kernels_run": bs.precision,
+                          "roofline": {"bound": "fp64" if bs.precision == "f64" else "fp32", "achieved": ach,
+                                       "peak": peak[bs.precision], "unit": "TFLOP/s", "frac": ach / peak[bs.precision],
                                        "traffic": None, "peak_source": "measured live by pe_pipe_probe",
                                        "flops_per_launch": flops},
+                          "bytes_roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+                                             "frac": gbs / hbm, "peak_source": hbm_src,
+                                             "bytes_per_launch": nbytes,
+                                             "note": "algorithmic bytes of the draws and block gathers (16 m k + "
+                                                     "16 k^2 per chain step); the instances are L2-resident"},
                           "clocks": clk.summary()}
         # end to end: the same batch with the occupations copied to pinned host memory every step
         host = torch.empty_like(bs.occ, device="cpu").pin_memory()
@@ -759,7 +779,7 @@ def main():
                     help="c2 (default) is the headline line; c1 c3 c4 c5 run through the batched sampler, emitter "
                          "the EmitterMPS path, single the one-sample latency path, adaptive prefix / avoid, published "
                          "the workloads of the reference's published H100 numbers")
-    ap.add_argument("--profile-launch", choices=("f64", "mixed"), default=None,
+    ap.add_argument("--profile-launch", choices=FORMS, default=None,
                     help="run only two chain launches of the workload (a target for ncu -s 1 -c 1)")
     args = ap.parse_args()
     if args.profile_launch:

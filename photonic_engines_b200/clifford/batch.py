@@ -19,7 +19,7 @@ import torch
 
 from .. import _native as N
 from .. import autotune
-from .kernels import WARP_MAX_PHOTONS, default_tpl, pack_ragged, split_plan, use_warp_form
+from .kernels import WARP_MAX_PHOTONS, default_tpl, effective_precision, pack_ragged, split_plan, use_warp_form
 
 DEFAULT_CUTS = (20, 16)
 # tier cut points the autotuner tries (descending; the last tier <= 16 photons runs in the warp form)
@@ -69,13 +69,13 @@ class BatchedSampler:
         xs = _per_instance(indist, G, 1.0)
         if any(not 0.0 <= e <= 1.0 for e in etas) or any(not 0.0 <= x <= 1.0 for x in xs):
             raise ValueError("loss (transmission) and indist (x-model overlap) must lie in [0, 1]")
-        self.precision = precision
         self.G = G
         self.shots = shots_l
         self.m = [int(U.shape[0]) for U, _ in circuits]
         self.n = [len(modes) for _, modes in circuits]
         self.m_max, self.n_stride = max(self.m), max(max(self.n), 1)
         N.check_photons(self.n_stride, precision, "photons per circuit")
+        self.precision = precision = effective_precision(precision, self.n_stride)
         self.S = sum(shots_l)
         self.acol, self.inst_off, self.inst_m, self.inst_n = pack_ragged(circuits)
         self.acol = torch.view_as_real(self.acol).contiguous()

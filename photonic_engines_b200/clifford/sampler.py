@@ -100,8 +100,10 @@ def fock_sample(U, in_modes, shots, generator=None, algo="auto", multi_min_k1=10
     "triton" and "cuda" are accepted and run the same kernels); algo: any of the reference's algorithms —
     they all draw the same chain, which is what runs.  multi_min_k1 / max_lanes / target_total_lanes /
     single_lanes are the reference's kernel tuning knobs and have no effect here.
-    precision: "f64" (complex FP64, the drop-in) or "mixed" (FP32 Gray blocks with FP64 cross-block sums,
-    marginals and CDF).  uniforms: optional float64 [S, n] per-step uniforms replacing the Philox draws
+    precision: "f64" (complex FP64, the drop-in), "mixed" (FP32 Gray blocks with FP64 cross-block sums,
+    marginals and CDF; ~1e-5 marginals at 20 photons; chains of at most 8 photons run the FP64 kernels, which
+    are faster there) or "compensated" (double-float FP32 Gray blocks: FP64-level marginals); every form
+    returns the FP64 form's samples.  uniforms: optional float64 [S, n] per-step uniforms replacing the Philox draws
     (lossless only).  stats: receives "passes" = [(k, streams, seconds)] — all passes run in one launch, so
     every entry carries that launch's time — and "fused_seconds".
     prefix (adaptive sampling, lossless only): the output modes the FIRST c photons of every chain are forced

@@ -996,14 +996,15 @@ template <class SM>
 static __device__ void draw_step(SM& sm, double* __restrict__ wgt, const double2* __restrict__ A, int64_t rs, int64_t cs,
                                  int m, int k, double u, double* __restrict__ marg_row, bool update_groups) {
     const int tid = threadIdx.x, T = blockDim.x, lid = tid & 31, wid = tid >> 5, nw = T >> 5;
-    // DR modes per thread at a time, so that DR independent loads of A (from L2) are in flight per
-    // column instead of one; the sum over columns keeps its order (same bits as one mode at a time)
+    // DR modes per thread at a time, and the column loop unrolled 4 times, so that 16 independent loads of
+    // A (from L2) are in flight instead of one; the sum over columns keeps its order (same bits as one mode
+    // at a time).  The draw is bound by L2 latency, not by its few FLOPs.
     constexpr int DR = 4;
     for (int rho0 = tid; rho0 < m; rho0 += T * DR) {
         double xr[DR], xi[DR];
 #pragma unroll
         for (int r = 0; r < DR; ++r) { xr[r] = 0.0; xi[r] = 0.0; }
-#pragma unroll 2
+#pragma unroll 4
         for (int c = 0; c < k; ++c) {
             const int64_t co = (int64_t)sm.cols[c] * cs;
             const double2 p = sm.P[c];

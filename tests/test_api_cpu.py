@@ -68,4 +68,8 @@ def test_photon_limits_are_checked_on_the_host():
         N.check_photons(33, "mixed")
     from photonic_engines_b200.clifford.kernels import default_tpl
     assert [default_tpl(n, "f64") for n in (6, 18, 24, 32, 36, 48, 64)] == [1, 1, 2, 2, 2, 4, 4]
-    assert [default_tpl(n, "mixed") for n in (6, 18, 24, 32)] == [1, 2, 2, 2]
+    assert [default_tpl(n, "mixed") for n in (6, 18, 24, 32)] == [1, 1, 2, 2]
+    assert [default_tpl(n, "compensated") for n in (6, 18, 24, 32)] == [1, 2, 4, 4]
+    N.check_photons(32, "compensated")
+    with pytest.raises(ValueError, match="compensated"):
+        N.check_photons(33, "compensated")
