@@ -90,6 +90,46 @@ def exact_distribution(U, ops, modes, s0, final=None) -> dict:
     return {k_: v / tot for k_, v in dist.items()}
 
 
+def subset_distribution(U, ops, modes, s0, final, T) -> dict:
+    """{occupation: probability} of the photons in slots T with every other photon traced out (lost):
+    P(o) = sum_{x, y} rho_T[x, y] per(U[rows(o), modes_T(x)]) conj(per(U[rows(o), modes_T(y)])) / prod o!,
+    rho_T the reduced density of the label tensor over T (a traced emitter's spin traced with the rest)."""
+    U = np.asarray(U, dtype=np.complex128)
+    m = U.shape[0]
+    ops = np.asarray(ops, dtype=np.complex128)
+    n, L, chi, _ = ops.shape
+    c = coefficient_tensor(ops, s0)
+    if final is not None:
+        c = np.einsum("...s,s->...", c, np.conj(np.asarray(final, dtype=np.complex128)))
+    T = list(T)
+    k = len(T)
+    rho_T = reduced_density(c, T)
+    xs = list(itertools.product(range(L), repeat=k))
+    dist = {}
+    for t in itertools.combinations_with_replacement(range(m), k):
+        occ = np.bincount(t, minlength=m)
+        pers = np.array([per_ryser(U[np.ix_(list(t), [modes[T[j]][x[j]] for j in range(k)])]) for x in xs])
+        p = float(np.einsum("x,xy,y->", pers, rho_T, pers.conj()).real)
+        dist[tuple(int(v) for v in occ)] = p / np.prod([math.factorial(int(v)) for v in occ])
+    tot = sum(dist.values())
+    return {k_: v / tot for k_, v in dist.items()}
+
+
+def lossy_distribution(U, ops, modes, s0, final, eta: float) -> dict:
+    """Law under uniform input-side loss: every photon survives independently with probability eta, the
+    lost ones are traced out (the reference's docs/LOSS.md model for emitters)."""
+    n = np.asarray(ops).shape[0]
+    m = np.asarray(U).shape[0]
+    dist: dict = {}
+    for r in range(n + 1):
+        for T in itertools.combinations(range(n), r):
+            w = eta ** r * (1 - eta) ** (n - r)
+            part = subset_distribution(U, ops, modes, s0, final, T) if T else {tuple([0] * m): 1.0}
+            for k_, p in part.items():
+                dist[k_] = dist.get(k_, 0.0) + w * p
+    return dist
+
+
 def sample(U, ops, modes, s0, final, shots: int, generator) -> np.ndarray:
     """Occupations [shots, m], drawing from `generator` (a torch CPU generator) in the reference sampler's
     order: final spins (traced emitter), photon orders, then one multinomial per step and stream."""

@@ -76,8 +76,10 @@ def lookup(device, precision: str, workload: str):
 
 
 def tune(run, device, precision: str, n_tier: int, workload: str, reps: int = 2, force: bool = False,
-         candidates=None):
-    """run(tpl, block) performs one launch on the current stream.  Returns the fastest (tpl, block)."""
+         candidates=None, keep_first_within: float = 0.0):
+    """run(tpl, block) performs one launch on the current stream.  Returns the fastest (tpl, block); with
+    keep_first_within = f the first candidate (the default) is kept unless another one is faster by more than
+    the fraction f (timing noise must not move a choice)."""
     k = key(device, precision, workload)
     cache = _load()
     if not force and k in cache:
@@ -85,6 +87,7 @@ def tune(run, device, precision: str, n_tier: int, workload: str, reps: int = 2,
     best, best_ms = None, float("inf")
     if candidates is None:
         candidates = (COMP_CANDIDATES if precision == "compensated" else CANDIDATES)[n_tier]
+    first_ms = None
     for tpl, block in candidates:
         run(tpl, block)                                         # warm-up (module load, attribute set-up)
         times = []
@@ -96,8 +99,12 @@ def tune(run, device, precision: str, n_tier: int, workload: str, reps: int = 2,
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
         ms = min(times)
+        if first_ms is None:
+            first_ms = ms
         if ms < best_ms:
             best, best_ms = (tpl, block), ms
+    if keep_first_within > 0.0 and best_ms > first_ms * (1.0 - keep_first_within):
+        best = tuple(candidates[0])
     cache = _load()
     cache[k] = list(best)
     _store(cache)

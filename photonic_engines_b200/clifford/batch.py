@@ -115,6 +115,7 @@ class BatchedSampler:
         self.tiered = bool(tiers and varied and not self.warp and not self.split and self.n_stride > WARP_MAX_PHOTONS)
         self.wsb = int(N.load().pe_chain_workspace_bytes(C))
         self.qr_all = torch.tensor([0, C], dtype=torch.int64, device=dev)      # the whole queue (warp form)
+        self.tier_ws, self._side_streams = [], []
         self._set_tiers(DEFAULT_CUTS if self.tiered else ())
         self.gen = torch.Generator(device=dev).manual_seed(seed)
         self._row0 = [0]
@@ -145,8 +146,12 @@ class BatchedSampler:
         self.tier_thr = torch.tensor([t[0] for t in self.tiers[1:]], dtype=torch.int32, device=dev)
         self.qr = torch.zeros(len(self.tiers), 2, dtype=torch.int64, device=dev)
         self.qr[-1, 1] = self.C                                      # the cuts between tiers move per batch
-        self.tier_ws = [torch.zeros(self.wsb, dtype=torch.uint8, device=dev) for _ in self.tiers]
-        self.tier_streams = [torch.cuda.Stream(dev) for _ in self.tiers[1:]]
+        # workspaces and side streams are made once, as many as the most tiers any cut set gives, and reused
+        while len(self.tier_ws) < len(self.tiers):
+            self.tier_ws.append(torch.zeros(self.wsb, dtype=torch.uint8, device=dev))
+        while len(self._side_streams) < len(self.tiers) - 1:
+            self._side_streams.append(torch.cuda.Stream(dev))
+        self.tier_streams = self._side_streams[:len(self.tiers) - 1]
 
     # ---------------------------------------------------------------------------------------- one batch
     def _draw_keys(self):
@@ -222,10 +227,11 @@ class BatchedSampler:
         self._partition()
 
         def run(i, _block):
-            self._set_tiers(cands[i])
+            if self.cuts != tuple(c for c in cands[i] if c < self.n_stride):   # switched in the warm-up call
+                self._set_tiers(cands[i])
             self._chains()
         best = autotune.tune(run, self.device, self.precision, 0, workload,
-                             candidates=[(i, 0) for i in range(len(cands))])
+                             candidates=[(i, 0) for i in range(len(cands))], reps=3, keep_first_within=0.03)
         self._set_tiers(cands[best[0]])
 
     def _autotune(self):
@@ -279,7 +285,7 @@ class BatchedSampler:
         """Raise when a device-side index error was recorded (synchronises)."""
         st = self.status.cpu().tolist()
         ws = 0
-        for w in (self.tier_ws if self.tiers else [self.ws]):
+        for w in (self.tier_ws[:len(self.tiers)] if self.tiers else [self.ws]):
             ws = ws or N.read_status(w)[0]
         if any(st) or ws:
             raise N.NativeError(f"device-side error in the batched sampler (partition {st[0]}, scatter {st[1]}, "

@@ -396,20 +396,218 @@ def step_weights(U_t: torch.Tensor, state: EmitterMPS, Tsorted: torch.Tensor, ro
     return w, nl
 
 
+# ---------------------------------------------------------------------------------------- loss / indist
+def slot_outcomes(state: EmitterMPS, fates: torch.Tensor, U: torch.Tensor, generator: torch.Generator,
+                  unravel: bool = True) -> tuple[torch.Tensor, torch.Tensor]:
+    """What is fixed before the chain rule runs on the interfering photons, slot by slot on the host:
+    the label of every lost slot (unravel=True: the trace over a lost photon's label is sampled, so the slot
+    becomes the single operator M_{j,x}) and the output row of every lone photon (it interferes with
+    nothing, so its row r is drawn from the exact marginal and the slot becomes G_j(r) = sum_l U[r, mode(j,
+    l)] M_{j,l}), then the final spin of a traced emitter given those outcomes.  Restates the reference's
+    emitter_terms.sample_slot_outcomes (photonic_engines/clifford/emitter_terms.py:71-137) and uses the
+    generator as it does: per slot, one multinomial over every stream's label weights when a stream lost
+    that slot, one over every stream's row weights when a stream has a lone photon there; last, one over
+    the final-spin weights.  Weights: Re Tr(E_{j+1} K rho K^dag) with E the traced environment of the later
+    slots and rho the forward register state (interfering slots summed over).
+
+    fates [S, n] (imperfections codes: LOST, LONE, 1 = interfering).  Returns (labels [S, n] int64: -1
+    summed over, x < L a lost slot's label, L + r a lone photon's row; fid [S] final-spin ids)."""
+    from ..imperfections import LONE, LOST
+    S, n = fates.shape
+    chi, L = state.chi, state.num_labels
+    ops = torch.as_tensor(state.ops, dtype=C128)
+    lost = (fates == LOST) if unravel else torch.zeros(S, n, dtype=torch.bool)
+    lone = fates == LONE
+    env = [None] * (n + 1)
+    env[n] = torch.eye(chi, dtype=C128) if state.final is None else torch.outer(
+        torch.as_tensor(state.final, dtype=C128), torch.as_tensor(state.final, dtype=C128).conj())
+    for j in range(n - 1, -1, -1):
+        env[j] = torch.einsum("lst,su,luv->tv", ops[j].conj(), env[j + 1], ops[j])
+    s0 = torch.as_tensor(state.s0, dtype=C128)
+    rho = torch.outer(s0, s0.conj()).expand(S, chi, chi).clone()
+    labels = torch.full((S, n), -1, dtype=torch.long)
+    Uh = torch.as_tensor(U).to("cpu", C128) if bool(lone.any()) else None
+    for j in range(n):
+        pair = torch.einsum("lts,xsu,kvu->xlktv", ops[j], rho, ops[j].conj())      # M_l rho M_k^dag
+        own = torch.einsum("xlltv->xltv", pair)                                    # [S, L, chi, chi]
+        nxt = own.sum(1)
+        if bool(lost[:, j].any()):
+            w = torch.einsum("tv,xlvt->xl", env[j + 1], own).real.clamp_min(0)
+            w = w / w.sum(1, keepdim=True).clamp_min(1e-300)
+            x = torch.multinomial(w, 1, generator=generator)[:, 0]
+            sel = lost[:, j]
+            labels[sel, j] = x[sel]
+            nxt = torch.where(sel.view(S, 1, 1), own[torch.arange(S), x], nxt)
+        if bool(lone[:, j].any()):
+            Um = Uh[:, list(state.modes[j])]                                          # [m, L]
+            byrow = torch.einsum("rl,rk,xlktv->xrtv", Um, Um.conj(), pair)           # G(r) rho G(r)^dag
+            w = torch.einsum("tv,xrvt->xr", env[j + 1], byrow).real.clamp_min(0)
+            w = w / w.sum(1, keepdim=True).clamp_min(1e-300)
+            r = torch.multinomial(w, 1, generator=generator)[:, 0]
+            sel = lone[:, j]
+            labels[sel, j] = L + r[sel]
+            nxt = torch.where(sel.view(S, 1, 1), byrow[torch.arange(S), r], nxt)
+        tr = torch.einsum("xtt->x", nxt).real.clamp_min(1e-300)
+        rho = nxt / tr.view(S, 1, 1)
+    if state.final is None:
+        pf = torch.einsum("xtt->xt", rho).real.clamp_min(0)
+        fid = torch.multinomial(pf / pf.sum(1, keepdim=True), 1, generator=generator)[:, 0]
+    else:
+        fid = torch.zeros(S, dtype=torch.long)
+    return labels, fid
+
+
+def fixed_slot_state(state: EmitterMPS, labels_row, U: torch.Tensor | None) -> EmitterMPS:
+    """The state a stream's chain runs on once its slot outcomes are fixed: a lost slot with label x keeps
+    the single operator M_{j,x}, a lone photon's slot with row r the operator sum_l u_l M_{j,l} with
+    u = U[r, mode(j, .)] / |U[r, mode(j, .)]| (a per-stream scale changes no conditional weight); both are
+    placed as label 0 with the other labels zero, so the slot is a one-operator channel wherever it is
+    traced.  Slots with label -1 are unchanged."""
+    ops = np.array(state.ops, dtype=np.complex128)
+    L = state.num_labels
+    Uh = None
+    for j, lab in enumerate(int(v) for v in labels_row):
+        if lab < 0:
+            continue
+        if lab < L:
+            wv = np.zeros(L, dtype=np.complex128)
+            wv[lab] = 1.0
+        else:
+            if Uh is None:
+                Uh = torch.as_tensor(U).to("cpu", C128).numpy()
+            wv = Uh[lab - L, list(state.modes[j])]
+            wv = wv / max(float(np.linalg.norm(wv)), 1e-300)
+        F = np.einsum("l,lts->ts", wv, ops[j])
+        ops[j] = 0.0
+        ops[j, 0] = F
+    return EmitterMPS(ops=ops, modes=state.modes, s0=state.s0, m=state.m, final=state.final)
+
+
+def _group_weights(U_t, ut, m, state: EmitterMPS, parts, T, rows_d, fid, modes32, ws):
+    """w [S, m] of one step for streams whose chains run on different fixed-slot states: parts = [(stream
+    indices, tables)], every stream in exactly one part; one pe_emitter_weights launch over all lanes."""
+    dev = U_t.device
+    S, k = T.shape
+    s0_l, mats_l, f_l, ls_l, nlan = [], [], [], [], torch.zeros(S, dtype=torch.int64, device=dev)
+    for idx, tb in parts:
+        s0, mats, f, _, nl_e = tb.lanes(T[idx], fid[idx])
+        s0_l.append(s0)
+        mats_l.append(mats)
+        f_l.append(f)
+        ls_l.append(torch.repeat_interleave(idx, nl_e))
+        nlan[idx] = nl_e
+    s0, mats, f = torch.cat(s0_l), torch.cat(mats_l), torch.cat(f_l)
+    lane_stream = torch.cat(ls_l)
+    nl = int(s0.shape[0])
+    # lanes of a stream are contiguous within its part; lstart points at each stream's first lane
+    first = torch.full((S,), -1, dtype=torch.int64, device=dev)
+    lane_idx = torch.arange(nl, device=dev)
+    first.scatter_reduce_(0, lane_stream, lane_idx, reduce="amin", include_self=False)
+    lstart = torch.where(nlan > 0, first, torch.zeros_like(first))
+    colmode = modes32[T].contiguous()
+    amp = torch.empty(max(nl, 1), m, dtype=C128, device=dev)
+    w = torch.empty(S, m, dtype=torch.float64, device=dev)
+    rc = N.load().pe_emitter_weights(N.ptr(ut), m, int(U_t.shape[1]), N.ptr(rows_d), int(rows_d.shape[1]),
+                                     N.ptr(colmode), S, k, state.num_labels, state.chi, N.ptr(torch.view_as_real(s0)),
+                                     N.ptr(torch.view_as_real(f)), N.ptr(torch.view_as_real(mats)), nl,
+                                     N.ptr(lane_idx), N.ptr(lane_stream), N.ptr(lstart), N.ptr(nlan), nl,
+                                     N.ptr(torch.view_as_real(amp)), N.ptr(w), N.ptr(ws), int(ws.numel()),
+                                     N.stream_handle(dev))
+    N.check(rc, "pe_emitter_weights")
+    return w, nl
+
+
+def _imperfect_sample(state: EmitterMPS, U_t: torch.Tensor, shots: int, generator, loss, indist,
+                      unravel: bool) -> torch.Tensor:
+    """emitter_sample under input-side loss and / or x-model partial distinguishability (the reference's
+    photonic_engines/clifford/__init__.py:62-128 with its torch sampler): photon fates on the generator
+    (imperfections.draw_fates), slot outcomes (`slot_outcomes`), then, for every count k of interfering
+    photons in ascending order, the chain rule over the k interfering slots of those streams — photon
+    order argsort(rand) over the kept slots, one multinomial per step — with every stream's lost and lone
+    slots fixed (`fixed_slot_state`); lone photons add their drawn rows to the occupations."""
+    from ..imperfections import LONE, draw_fates
+    dev = U_t.device
+    m, n, L = U_t.shape[0], state.n, state.num_labels
+    fates = draw_fates(n, shots, loss, indist, generator=generator)
+    good = fates == 1
+    labels = fid = None
+    if unravel or bool((fates == LONE).any()):
+        labels, fid = slot_outcomes(state, fates, U_t, generator, unravel)
+    occ = torch.zeros((shots, m), dtype=torch.long)
+    ut = torch.view_as_real(U_t.transpose(0, 1).contiguous()).contiguous()
+    modes32 = torch.tensor([list(mk) for mk in state.modes], dtype=torch.int32, device=dev)
+    ws = torch.empty(int(N.load().pe_emitter_workspace_bytes()), dtype=torch.uint8, device=dev)
+    kept = good.sum(1)
+    fixed: dict = {}                                                      # labels row -> (state, tables)
+    for k in torch.unique(kept).tolist():
+        if k == 0:
+            continue
+        ids = torch.nonzero(kept == k)[:, 0]
+        Sk = int(ids.shape[0])
+        keep = torch.arange(n).expand(Sk, n)[good[ids]].view(Sk, k)
+        if fid is not None:
+            fk = fid[ids]
+        elif state.final is None:
+            pf = final_spin_distribution(state)
+            fk = torch.multinomial(pf / pf.sum(), Sk, replacement=True, generator=generator)
+        else:
+            fk = torch.zeros(Sk, dtype=torch.long)
+        sigma = keep.gather(1, torch.argsort(torch.rand(keep.shape, generator=generator), dim=1))
+        # streams by the fixed-slot state their chains run on
+        rows_lab = labels[ids] if labels is not None else torch.full((Sk, n), -1, dtype=torch.long)
+        uniq, inv = torch.unique(rows_lab, dim=0, return_inverse=True)
+        parts = []
+        for u_i, row in enumerate(uniq.tolist()):
+            key = tuple(row)
+            if key not in fixed:
+                st = state if all(v < 0 for v in row) else fixed_slot_state(state, row, U_t)
+                fixed[key] = (st, tables_for(st, dev))
+            parts.append((torch.nonzero(inv == u_i)[:, 0].to(dev), fixed[key][1]))
+        fk_d = fk.to(dev)
+        rows = torch.zeros((Sk, k), dtype=torch.long)
+        rows_d = torch.zeros((Sk, max(k, 1)), dtype=torch.int64, device=dev)
+        for step in range(1, k + 1):
+            T = torch.sort(sigma[:, :step], dim=1).values.to(dev)
+            w, _ = _group_weights(U_t, ut, m, state, parts, T, rows_d, fk_d, modes32, ws)
+            w = w.cpu().clamp_min(0)
+            w = w / w.sum(dim=1, keepdim=True)
+            rho = torch.multinomial(w, 1, generator=generator).squeeze(1)
+            rows[:, step - 1] = rho
+            rows_d[:, step - 1] = rho.to(dev)
+        st_, det = N.read_status(ws)
+        if st_ != 0:
+            raise N.NativeError(f"pe_emitter_weights: device-side index error at {det}")
+        part_occ = torch.zeros((Sk, m), dtype=torch.long)
+        part_occ.scatter_add_(1, rows, torch.ones_like(rows))
+        occ[ids] = part_occ
+    if labels is not None:                                                 # lone photons: their drawn rows
+        s_, j_ = torch.nonzero(fates == LONE, as_tuple=True)
+        occ.index_put_((s_, labels[s_, j_] - L), torch.ones_like(s_), accumulate=True)
+    return occ.to(dev)
+
+
 def emitter_sample(state: EmitterMPS, U: torch.Tensor, shots: int, generator: torch.Generator | None = None,
-                   backend: str = "b200", return_stats: bool = False, loss=None, indist=None, **kw):
+                   backend: str = "b200", return_stats: bool = False, loss=None, indist=None, unravel: bool = True,
+                   **kw):
     """Exact samples [shots, m] int64 (on U's device) of the EmitterMPS `state` through U (CUDA).
 
     Keeps the reference's call (photonic_engines/clifford/__init__.py:36-60) and the random-number use of
     its exact torch sampler (emitter_sampler.py:100-180): a final emitter spin per stream from p(s_f) when
     the emitter is traced out (multinomial on `generator`), the photon order argsort(rand(shots, n)), then
     one multinomial draw per step from the normalised weights — with a CPU generator seeded alike, the
-    same samples.  chi = 2 and 1 or 2 labels per photon (the reference GPU kernel's range); loss and
-    partial distinguishability are not part of this path."""
+    same samples.  chi = 2 and 1 or 2 labels per photon (the reference GPU kernel's range).
+    loss: uniform input-side transmission; indist: x-model partial distinguishability (a float x, or the
+    model); unravel: sample lost photons' labels (one pure term per gap, the reference's default) instead
+    of tracing them — both as the reference's emitter_sample (photonic_engines/clifford/__init__.py:36-128),
+    with its draws when the generator is a CPU generator."""
+    from ..imperfections import as_model, transmission
     if backend not in ("b200", "triton", "torch", "cuda"):
         raise ValueError(f"unknown backend {backend!r}")
-    if loss is not None and float(loss) < 1.0 or indist is not None:
-        raise NotImplementedError("emitter_sample: loss / partial distinguishability are not available on this path")
+    model = as_model(indist)
+    eta = transmission(loss)
+    if model is not None and model.species is not None:
+        raise NotImplementedError("emitter_sample: partial distinguishability is the x-model only (several "
+                                  "interfering species would need a multi-species chain rule)")
     state.require_uniform_labels("emitter_sample")
     if state.chi != 2 or state.num_labels > 2:
         raise NotImplementedError("emitter_sample: emitter dimension 2 with 1 or 2 labels per photon only")
@@ -424,6 +622,13 @@ def emitter_sample(state: EmitterMPS, U: torch.Tensor, shots: int, generator: to
     S = int(shots)
     if generator is None:
         generator = torch.Generator().manual_seed(0)
+    if eta is not None or model is not None:
+        if return_stats:
+            raise NotImplementedError("emitter_sample: return_stats with loss / indist")
+        if generator.device.type != "cpu":                    # the host draws need a CPU generator
+            seed = int(torch.randint(0, 2 ** 31 - 1, (1,), generator=generator, device=generator.device).item())
+            generator = torch.Generator().manual_seed(seed)
+        return _imperfect_sample(state, U_t, S, generator, eta, model, unravel)
     gdev = generator.device
     if state.final is None:
         pf = final_spin_distribution(state)

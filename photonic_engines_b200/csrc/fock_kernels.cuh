@@ -998,7 +998,8 @@ static __device__ void draw_step(SM& sm, double* __restrict__ wgt, const double2
     const int tid = threadIdx.x, T = blockDim.x, lid = tid & 31, wid = tid >> 5, nw = T >> 5;
     // DR modes per thread at a time, and the column loop unrolled 4 times, so that 16 independent loads of
     // A (from L2) are in flight instead of one; the sum over columns keeps its order (same bits as one mode
-    // at a time).  The draw is bound by L2 latency, not by its few FLOPs.
+    // at a time).  The draw is bound by L2 latency, not by its few FLOPs (m = 900, the c3 batch: 4-5 %
+    // faster than two columns ahead).
     constexpr int DR = 4;
     for (int rho0 = tid; rho0 < m; rho0 += T * DR) {
         double xr[DR], xi[DR];

@@ -2,7 +2,7 @@
 
 Run in a container where the reference project is importable (it is NOT needed at test time):
 
-    python tests/golden/make_golden.py /path/to/photonic-engines [philox steps chains adaptive emitter slos]
+    python tests/golden/make_golden.py /path/to/photonic-engines [philox steps chains adaptive emitter slos emitter_imperfect]
 
 It imports the reference read-only and records, with CPU tensors and the Triton CPU interpreter:
 
@@ -21,6 +21,8 @@ It imports the reference read-only and records, with CPU tensors and the Triton 
   emitter.npz  EmitterMPS inputs (chi = 2): step weights of `emitter_reference.matrix_cofactor_weights`
                (emitter_reference.py:280-305) and occupations drawn by the exact torch sampler
                `emitter_sampler.sample_torch` (emitter_sampler.py:82-180) for seeded CPU generators.
+  emitter_imperfect.npz  EmitterMPS occupations of the reference's emitter_sample with loss and partial
+               distinguishability, and its slot outcomes (lost labels, lone rows, final spin).
   slos.npz     exact output probabilities of small circuits from the reference's SLOS kernel
                (slos/kernel.py:83-285): lossless, bunched input, x-model and lossy cases.
   chains.npz   whole chains drawn by the reference's sampler: `_sample_streams`
@@ -310,6 +312,43 @@ def make_emitter():
     np.savez_compressed(os.path.join(HERE, "emitter.npz"), **out)
 
 
+# (emitter, loss eta or None, x-model overlap or None, unravel): imperfect emitter draws recorded
+EMITTER_IMPERFECT = [("rand_n4_L2_t", 0.7, None, True), ("rand_n4_L2_t", None, 0.8, True),
+                     ("rand_n5_L2_f", 0.8, 0.9, True), ("caterpillar_n5", 0.75, None, True),
+                     ("caterpillar_n5", 0.7, None, False), ("rand_n5_L1_t", 0.85, 0.85, True)]
+
+
+def make_emitter_imperfect():
+    """emitter_imperfect.npz: occupations of the reference's emitter_sample with loss and / or x-model
+    partial distinguishability (photonic_engines/clifford/__init__.py:36-128, backend "torch", seeded CPU
+    generators), and the slot outcomes of emitter_terms.sample_slot_outcomes (emitter_terms.py:71-137) for
+    recorded fates (0 lost, 1 lone, 2 interfering)."""
+    from photonic_engines.clifford import emitter_sample
+    from photonic_engines.clifford.emitter_terms import sample_slot_outcomes
+    states = dict(_emitters())
+    out = {}
+    for ci, (name, eta, x, unravel) in enumerate(EMITTER_IMPERFECT):
+        st = states[name]
+        U = haar(st.m, 700 + ci)
+        case = f"c{ci}"
+        out[f"{case}__name"] = np.array(name)
+        out[f"{case}__U"] = U.numpy()
+        out[f"{case}__imperf"] = np.array([-1.0 if eta is None else eta, -1.0 if x is None else x, float(unravel)])
+        shots, seed = 200, 40 + ci
+        occ = emitter_sample(st, U, shots, generator=torch.Generator().manual_seed(seed), backend="torch",
+                             loss=eta, indist=x, unravel=unravel)
+        out[f"{case}__shots_seed"] = np.array([shots, seed])
+        out[f"{case}__occ"] = occ.numpy()
+        rng = np.random.default_rng(90 + ci)
+        roles = torch.as_tensor(rng.choice([0, 1, 2], size=(64, st.n), p=[0.3, 0.2, 0.5]), dtype=torch.long)
+        labels, fid = sample_slot_outcomes(st, roles, U, generator=torch.Generator().manual_seed(seed + 1))
+        out[f"{case}__roles"] = roles.numpy()
+        out[f"{case}__labels"] = labels.numpy()
+        out[f"{case}__fid"] = fid.numpy()
+        print(case, name, eta, x, unravel, tuple(occ.shape), int(occ.sum()), flush=True)
+    np.savez_compressed(os.path.join(HERE, "emitter_imperfect.npz"), **out)
+
+
 # (name, m, input modes, Haar seed, loss eta or None, x-model overlap or None): the small cases whose exact
 # law the tests compare samples with (histogram TVD tests), lossless, lossy and partially distinguishable
 SLOS_CASES = [("m4_n3", 4, [0, 1, 2], 104, None, None), ("m5_bunched", 5, [0, 0, 1], 105, None, None),
@@ -353,5 +392,5 @@ if __name__ == "__main__":
     parts = sys.argv[2:] or ["philox", "steps", "chains", "adaptive"]
     for part in parts:
         {"philox": make_philox, "steps": make_steps, "chains": make_chains, "adaptive": make_adaptive,
-         "emitter": make_emitter, "slos": make_slos}[part]()
+         "emitter": make_emitter, "slos": make_slos, "emitter_imperfect": make_emitter_imperfect}[part]()
         print(part, "done", flush=True)

@@ -107,8 +107,11 @@ def test_emitter_state_checks():
 def test_emitter_sample_argument_checks():
     st, U, *_ = case("rand_n3_L2_f")
     U = torch.as_tensor(U)
-    with pytest.raises(NotImplementedError):
-        emitter_sample(st, U, 4, loss=0.5)
+    from photonic_engines_b200.imperfections import Distinguishability
+    with pytest.raises(NotImplementedError):                       # several interfering species
+        emitter_sample(st, U, 4, indist=Distinguishability(species=(0.5, 0.3)))
+    with pytest.raises(ValueError):
+        emitter_sample(st, U, 4, loss=1.5)
     with pytest.raises(NotImplementedError):
         emitter_sample(EmitterMPS(ops=np.zeros((2, 1, 3, 3)), modes=((0,), (1,)), s0=[1, 0, 0], m=3), U[:3, :3], 2)
     with pytest.raises(ValueError):
@@ -135,3 +138,32 @@ def test_batched_lanes_are_the_per_set_terms(final):
             _, a0, am, af = gap_terms(st, T[s].tolist(), fv)
             sl = slice(int(lstart[s]), int(lstart[s] + nlan[s]))
             assert torch.equal(a0, s0[sl]) and torch.equal(am, mats[sl]) and torch.equal(af, f[sl]), (k, s)
+
+
+IMP = np.load(os.path.join(GOLDEN, "emitter_imperfect.npz"))
+IMP_CASES = sorted({k.split("__")[0] for k in IMP.files})
+
+
+@pytest.mark.parametrize("c", IMP_CASES)
+def test_slot_outcomes_reproduce_the_reference_draws(c):
+    """Lost labels, lone photons' rows and the final spin drawn slot by slot (the reference's
+    emitter_terms.sample_slot_outcomes on recorded fates, seeded CPU generator): the same values."""
+    from photonic_engines_b200.clifford.emitter import slot_outcomes
+    st, *_ = case(str(IMP[f"{c}__name"]))
+    U = torch.as_tensor(IMP[f"{c}__U"])
+    fates = torch.as_tensor(IMP[f"{c}__roles"]) - 1                  # reference 0 / 1 / 2 -> LOST / LONE / 1
+    seed = int(IMP[f"{c}__shots_seed"][1])
+    labels, fid = slot_outcomes(st, fates, U, torch.Generator().manual_seed(seed + 1))
+    assert np.array_equal(labels.numpy(), IMP[f"{c}__labels"])
+    assert np.array_equal(fid.numpy(), IMP[f"{c}__fid"])
+
+
+def test_fixed_slot_state_keeps_one_operator_per_fixed_slot():
+    from photonic_engines_b200.clifford.emitter import fixed_slot_state
+    st, U, *_ = case("rand_n4_L2_t")
+    fx = fixed_slot_state(st, [-1, 1, 2 + 3, -1], torch.as_tensor(U))
+    assert np.allclose(fx.ops[0], st.ops[0]) and np.allclose(fx.ops[3], st.ops[3])
+    assert np.allclose(fx.ops[1, 0], st.ops[1, 1]) and not fx.ops[1, 1].any()
+    u = U[3, list(st.modes[2])]
+    assert np.allclose(fx.ops[2, 0], np.einsum("l,lts->ts", u / np.linalg.norm(u), st.ops[2]))
+    assert not fx.ops[2, 1].any()

@@ -140,3 +140,35 @@ def test_fused_steps_match_the_oracle(n, L, ks, final):
             colmode = np.array([list(st.modes[j]) for j in kept])
             want = EO.matrix_weights(U, colmode, rows[s, :k - 1].tolist(), s0.numpy(), mats.numpy(), f.numpy())
             assert _rel(got[s], want) < 1e-10, (n, L, k, s)
+
+
+# ------------------------------------------------------------------------------------------- loss / indist
+from test_emitter_cpu import IMP, IMP_CASES  # noqa: E402
+
+
+@pytest.mark.parametrize("c", IMP_CASES)
+def test_imperfect_emitter_samples_reproduce_the_reference(c):
+    """Loss and x-model partial distinguishability (lost labels unravelled or traced, lone photons' rows,
+    chains over the interfering slots grouped by count): a seeded CPU generator gives the occupations the
+    reference's emitter_sample recorded."""
+    st, *_ = case(str(IMP[f"{c}__name"]))
+    U = torch.as_tensor(IMP[f"{c}__U"], device=DEV)
+    eta, x, unravel = IMP[f"{c}__imperf"].tolist()
+    shots, seed = (int(v) for v in IMP[f"{c}__shots_seed"])
+    occ = emitter_sample(st, U, shots, generator=torch.Generator().manual_seed(seed),
+                         loss=None if eta < 0 else eta, indist=None if x < 0 else x, unravel=bool(unravel))
+    assert np.array_equal(occ.cpu().numpy(), IMP[f"{c}__occ"])
+
+
+def test_lossy_emitter_law_matches_the_exact_mixture():
+    """A lossy traced emitter (n = 4, 2 labels): the sampled law against the exact mixture over the
+    surviving photons' reduced states (oracle: each survivor subset weighted eta^|T| (1 - eta)^(n - |T|),
+    the explicit reduced density matrix of T and Ryser permanents)."""
+    st, U, *_ = case("rand_n4_L2_t")
+    eta, shots = 0.6, 30000
+    dist = EO.lossy_distribution(U, st.ops, st.modes, st.s0, st.final, eta)
+    assert abs(sum(dist.values()) - 1.0) < 1e-9
+    occ = emitter_sample(st, torch.as_tensor(U, device=DEV), shots, generator=torch.Generator().manual_seed(3),
+                         loss=eta)
+    tvd, floor = O.tvd_and_floor(dist, occ.cpu().numpy())
+    assert tvd < 2.5 * floor, (tvd, floor)
