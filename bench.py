@@ -120,7 +120,9 @@ def run_reference(args):
     A = U[:, :N_PHOT]
     threads = os.cpu_count() or 1
     rng = np.random.default_rng(0)
-    S = args.ref_shots or 32 * threads          # about 4-5 s of work per step on this port
+    # the benchmark's own 2 000 chains per step when the whole run stays near 150 s on this port (about 17
+    # chains/s per host thread at n = 20, m = 400), else fewer per step
+    S = args.ref_shots or max(64, min(SHOTS, int(150 * 17 * threads / max(1, args.steps + args.warmup))))
 
     def step():
         sig = np.argsort(rng.random((S, N_PHOT)), axis=1)
@@ -137,7 +139,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "samples/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": N_PHOT, "m": M_MODES, "shots_per_step": S},
+            "config": {"workload": WORKLOAD, "n": N_PHOT, "m": M_MODES, "shots_per_step": S, "precision": "f64"},
             "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "port",
                              "sample": f"{S} chains per step of the n=20 m=400 workload (bounded sample)"},
             "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
