@@ -141,6 +141,28 @@ int pe_fock_chain_range(int precision, const double* d_acol, const int64_t* d_in
                         int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
                         int grid_ctas, const int64_t* d_qrange, int nk_max, int warp, void* stream);
 
+/*
+ * One tier of a length-sorted batch, as pe_fock_chain_range (CTA form), with the heavy steps of its first
+ * split_slots queue positions spread over nch CTAs per stream: the persistent kernel runs those positions'
+ * steps 1..k_split-1 and every later position's whole chain; then every step k = k_split..nk_max runs the
+ * split kernels over the slots (slot q = queue position q of the range, nothing past its end).  For the
+ * longest chains of a ragged batch (a lossy batch's few 25-30-photon survivors), which would otherwise
+ * each hold one CTA for the whole batch.  Workspace: pe_range_split_workspace_bytes(split_slots, nch).
+ * No counterpart in the reference (its lossy passes run one launch grid per surviving count,
+ * photonic_engines/clifford/sampler.py:188-215).
+ */
+int pe_fock_chain_range_split(int precision, const double* d_acol, const int64_t* d_inst_off,
+                              const int32_t* d_inst_m, const int32_t* d_inst_n, int G, int m_max, int64_t S,
+                              const int64_t* d_dp, const int32_t* d_nk, const int64_t* d_cols, int n_stride,
+                              const double* d_uniforms, const int64_t* d_seeds, const int64_t* d_seed_row,
+                              const int64_t* d_rng_off, const int64_t* d_order, int64_t* d_rows, int64_t* d_occ,
+                              int occ_stride, double* d_marg, int marg_stride, void* d_workspace,
+                              size_t workspace_bytes, int block_threads, int tpl, const int64_t* d_qrange,
+                              int nk_max, int k_split, int nch, int64_t split_slots, void* stream);
+
+/* Bytes of device workspace pe_fock_chain_range_split needs for split_slots slots of nch CTAs each. */
+size_t pe_range_split_workspace_bytes(int64_t split_slots, int nch);
+
 /* Bytes of device workspace pe_fock_chain_split needs for S streams and nch CTAs per stream. */
 size_t pe_chain_split_workspace_bytes(int64_t S, int nch);
 

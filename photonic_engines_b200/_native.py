@@ -73,6 +73,12 @@ def load() -> ctypes.CDLL:
     L.pe_fock_chain_range.argtypes = [_i32, _vp, _vp, _vp, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i32, _vp, _vp, _vp,
                                       _vp, _vp, _vp, _vp, _i32, _vp, _i32, _vp, ctypes.c_size_t, _i32, _i32, _i32,
                                       _vp, _i32, _i32, _vp]
+    L.pe_fock_chain_range_split.restype = _i32
+    L.pe_fock_chain_range_split.argtypes = [_i32, _vp, _vp, _vp, _vp, _i32, _i32, _i64, _vp, _vp, _vp, _i32, _vp, _vp,
+                                            _vp, _vp, _vp, _vp, _vp, _i32, _vp, _i32, _vp, ctypes.c_size_t, _i32,
+                                            _i32, _vp, _i32, _i32, _i32, _i64, _vp]
+    L.pe_range_split_workspace_bytes.restype = ctypes.c_size_t
+    L.pe_range_split_workspace_bytes.argtypes = [_i64, _i32]
     L.pe_chain_split_workspace_bytes.restype = ctypes.c_size_t
     L.pe_chain_split_workspace_bytes.argtypes = [_i64, _i32]
     L.pe_fock_chain_adaptive.restype = _i32
@@ -118,7 +124,7 @@ def load() -> ctypes.CDLL:
 # every symbol the C header declares (checked by the CPU test that loads the library)
 EXPORTED = ("pe_version", "pe_max_modes", "pe_chain_workspace_bytes", "pe_fock_chain", "pe_fock_chain_noalloc",
             "pe_fock_chain_split", "pe_chain_split_workspace_bytes", "pe_split_slots", "pe_fock_chain_warp",
-            "pe_fock_chain_range",
+            "pe_fock_chain_range", "pe_fock_chain_range_split", "pe_range_split_workspace_bytes",
             "pe_fock_chain_adaptive", "pe_adaptive_workspace_bytes", "pe_emitter_weights",
             "pe_emitter_workspace_bytes", "pe_emitter_count", "pe_emitter_step",
             "pe_cofactors_rows", "pe_partition_shots", "pe_scatter_occupations", "pe_pipe_probe", "pe_read_status",

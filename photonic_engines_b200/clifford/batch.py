@@ -15,13 +15,22 @@ equivalent is one `fock_sample(..., loss=eta_g)` call per circuit.
 """
 from __future__ import annotations
 
+import math
+
 import torch
 
 from .. import _native as N
 from .. import autotune
-from .kernels import WARP_MAX_PHOTONS, default_tpl, effective_precision, pack_ragged, split_plan, use_warp_form
+from .kernels import (WARP_MAX_PHOTONS, _split_slots, default_tpl, effective_precision, pack_ragged, split_plan,
+                      use_warp_form)
+
+
+def _resident_split_ctas(device, precision: str, n: int, tpl: int) -> int:
+    dev = torch.device(device)
+    return _split_slots(dev.index if dev.index is not None else torch.cuda.current_device(), precision, n, 128, tpl)
 
 DEFAULT_CUTS = (20, 16)
+LONG_SPLIT_ABOVE = 24          # chains longer than this get their own tier with split steps
 # tier cut points the autotuner tries (descending; the last tier <= 16 photons runs in the warp form)
 CUT_CANDIDATES = [(20, 16), (24, 16), (20, 12), (24, 20, 16), (16,), (20, 16, 12)]
 
@@ -116,6 +125,7 @@ class BatchedSampler:
         self.wsb = int(N.load().pe_chain_workspace_bytes(C))
         self.qr_all = torch.tensor([0, C], dtype=torch.int64, device=dev)      # the whole queue (warp form)
         self.tier_ws, self._side_streams = [], []
+        self.long_split = self._plan_long_split(etas, xs) if self.tiered else None
         self._set_tiers(DEFAULT_CUTS if self.tiered else ())
         self.gen = torch.Generator(device=dev).manual_seed(seed)
         self._row0 = [0]
@@ -123,6 +133,7 @@ class BatchedSampler:
             self._row0.append(self._row0[-1] + s_)
         self.tpl, self.block = tpl, block_threads
         self.warp_block = 0                                          # streams per CTA of a warp-form tier x 32
+        self.graph = None
         if tune and self.tiered:
             self._tune_cuts()
         if tune and not (tpl and block_threads):
@@ -143,15 +154,51 @@ class BatchedSampler:
             return
         last_warp = 1 if (cuts[-1] <= WARP_MAX_PHOTONS and self.precision != "compensated") else 0
         self.tiers = [(self.n_stride, 0)] + [(c, 0) for c in cuts[:-1]] + [(cuts[-1], last_warp)]
+        if self.long_split is not None:                  # the longest chains: their own tier, steps split
+            lim = self.long_split["above"]
+            self.tiers = [(self.n_stride, 2)] + [t for t in self.tiers if t[0] < lim]
+            if self.tiers[1][0] != lim:
+                self.tiers.insert(1, (lim, 0))
         self.tier_thr = torch.tensor([t[0] for t in self.tiers[1:]], dtype=torch.int32, device=dev)
         self.qr = torch.zeros(len(self.tiers), 2, dtype=torch.int64, device=dev)
         self.qr[-1, 1] = self.C                                      # the cuts between tiers move per batch
         # workspaces and side streams are made once, as many as the most tiers any cut set gives, and reused
+        if self.long_split is not None and not self.tier_ws:
+            self.tier_ws.append(torch.zeros(self.long_split["ws_bytes"], dtype=torch.uint8, device=dev))
         while len(self.tier_ws) < len(self.tiers):
             self.tier_ws.append(torch.zeros(self.wsb, dtype=torch.uint8, device=dev))
         while len(self._side_streams) < len(self.tiers) - 1:
             self._side_streams.append(torch.cuda.Stream(dev))
         self.tier_streams = self._side_streams[:len(self.tiers) - 1]
+
+    def _plan_long_split(self, etas, xs):
+        """The split tier of the longest chains (more than LONG_SPLIT_ABOVE photons), or None: expected count E
+        of such chains per batch (every photon of circuit g interferes with probability eta_g x_g), slots
+        4 E + 64 (positions past them run whole in the persistent kernel), nch a power of two with E nch at
+        least four times the split kernel's resident CTAs, k_split the first step with 4 nch lanes' worth of
+        Gray terms.  A chain of 27 photons holds one CTA for about 0.3 s, as long as all other chains of a
+        100 000-shot batch together; split, its heavy steps run on nch CTAs."""
+        above = LONG_SPLIT_ABOVE
+        if self.n_stride <= above:
+            return None
+        E = 0.0
+        for n_g, sh, e_, x_ in zip(self.n, self.shots, etas, xs):
+            q = e_ * x_
+            E += sh * sum(math.comb(n_g, j) * q ** j * (1.0 - q) ** (n_g - j) for j in range(above + 1, n_g + 1))
+        slots = int(min(self.C, 4 * E + 64))
+        tpl = default_tpl(self.n_stride, self.precision)
+        resident = _resident_split_ctas(self.device, self.precision, self.n_stride, tpl)
+        nch = 4
+        while nch < 128 and max(E, 1.0) * nch < 4 * resident:
+            nch *= 2
+        lanes = 128 // tpl
+        k = 2
+        while k <= self.n_stride and (1 << (k - 2)) < 4 * nch * lanes:
+            k += 1
+        if k > self.n_stride:
+            return None
+        wsb = int(N.load().pe_range_split_workspace_bytes(slots, nch))
+        return {"above": above, "slots": slots, "nch": nch, "k_split": k, "expected": E, "ws_bytes": wsb}
 
     # ---------------------------------------------------------------------------------------- one batch
     def _draw_keys(self):
@@ -184,13 +231,20 @@ class BatchedSampler:
             cur = torch.cuda.current_stream(self.device)
             for s_ in self.tier_streams:
                 s_.wait_stream(cur)
-            for i, (nk_max, warp) in enumerate(self.tiers):
+            for i, (nk_max, mode) in enumerate(self.tiers):
                 stream = cur if i == 0 else self.tier_streams[i - 1]
                 b, t = (block, tpl) if i == 0 else (0, 0)          # the tuned shape is the top tier's
-                if warp:
+                if mode == 1:
                     b, t = self.warp_block, 0
+                if mode == 2:
+                    ls = self.long_split
+                    rc = L.pe_fock_chain_range_split(*common, N.ptr(self.tier_ws[i]), self.tier_ws[i].numel(), b, t,
+                                                     N.ptr(self.qr[i]), nk_max, ls["k_split"], ls["nch"],
+                                                     ls["slots"], stream.cuda_stream)
+                    N.check(rc, "pe_fock_chain_range_split")
+                    continue
                 rc = L.pe_fock_chain_range(*common, N.ptr(self.tier_ws[i]), self.tier_ws[i].numel(), b, t, 0,
-                                           N.ptr(self.qr[i]), nk_max, warp, stream.cuda_stream)
+                                           N.ptr(self.qr[i]), nk_max, mode, stream.cuda_stream)
                 N.check(rc, "pe_fock_chain_range")
             for s_ in self.tier_streams:
                 cur.wait_stream(s_)
@@ -218,20 +272,22 @@ class BatchedSampler:
         self._scatter()
 
     def _tune_cuts(self):
-        """Pick the tier cut points: every candidate set is timed on this batch (partition drawn once), the
-        fastest kept and cached per GPU and workload like the launch shape."""
+        """Pick the tier cut points: every candidate set is captured as the batch's CUDA graph and timed by
+        whole-batch replays (the tiers run concurrently on their streams, so only the replayed graph times
+        them as they run), the fastest kept — the default unless another set is more than 3 % faster — and
+        cached per GPU and workload like the launch shape."""
         workload = (f"cuts|G{self.G}|S{self.S}|m{self.m_max}|n{self.n_stride}|singles{int(self.singles)}|"
                     f"{self.precision}")
         cands = [c for c in CUT_CANDIDATES if all(x < self.n_stride for x in c)] or [DEFAULT_CUTS]
-        self._draw_keys()
-        self._partition()
 
         def run(i, _block):
-            if self.cuts != tuple(c for c in cands[i] if c < self.n_stride):   # switched in the warm-up call
-                self._set_tiers(cands[i])
-            self._chains()
+            if self.graph is None or self.cuts != tuple(c for c in cands[i] if c < self.n_stride):
+                self._set_tiers(cands[i])                  # switched (and captured) in the warm-up call
+                self._capture()
+            self.graph.replay()
         best = autotune.tune(run, self.device, self.precision, 0, workload,
                              candidates=[(i, 0) for i in range(len(cands))], reps=3, keep_first_within=0.03)
+        self.graph = None
         self._set_tiers(cands[best[0]])
 
     def _autotune(self):

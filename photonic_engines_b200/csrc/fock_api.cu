@@ -257,9 +257,10 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
                         int marg_stride, void* d_workspace, size_t workspace_bytes, int block_threads, int tpl,
                         int grid_ctas, int k_split, int nch, void* stream, bool warp_mode = false,
                         int k_first = 1, int k_last = 0, bool zero_status = true,
-                        const int64_t* d_qrange = nullptr, int nk_max = 0) {
+                        const int64_t* d_qrange = nullptr, int nk_max = 0, int64_t split_slots = 0) {
     if (!prec_ok(precision)) return PE_ERR_ARG;
-    if (nk_max < 0 || nk_max > n_stride || (d_qrange && k_split > 0)) return PE_ERR_ARG;
+    if (nk_max < 0 || nk_max > n_stride || split_slots < 0) return PE_ERR_ARG;
+    if (d_qrange && k_split > 0 && split_slots < 1) return PE_ERR_ARG;      // a split range needs its slot count
     if (k_first < 1 || k_first > n_stride + 1 || k_last < 0) return PE_ERR_ARG;
     if (S < 0 || G < 1 || m_max < 1 || n_stride < 1) return PE_ERR_ARG;
     if (!d_acol || !d_inst_off || !d_inst_m || !d_inst_n || !d_dp || !d_cols || !d_rows || !d_workspace) return PE_ERR_ARG;
@@ -268,8 +269,10 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     if (d_marg && marg_stride < m_max) return PE_ERR_ARG;
     if (k_split < 0 || (k_split > 0 && (k_split < 2 || nch < 1))) return PE_ERR_ARG;
     const bool split = k_split > 0 && k_split <= n_stride;
-    const size_t part_bytes = split ? (size_t)S * nch * MAXN * sizeof(double2) : 0;
-    const size_t need = WS_BYTES + part_bytes + (split ? (size_t)S * sizeof(int) : 0);
+    // split slots: every stream, or (a queue range) its first split_slots positions
+    const int64_t nq = d_qrange ? (split_slots < S ? split_slots : S) : S;
+    const size_t part_bytes = split ? (size_t)nq * nch * MAXN * sizeof(double2) : 0;
+    const size_t need = WS_BYTES + part_bytes + (split ? (size_t)nq * sizeof(int) : 0);
     if (workspace_bytes < need || ((uintptr_t)d_workspace & 15u)) return PE_ERR_SIZE;
     const int ncols = nk_max > 0 ? nk_max : n_stride;        // the longest chain the launch may meet
     const int kpm = kpm_for(ncols);
@@ -331,6 +334,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     p.tau_log2g = 0.251;       // log2(1.19)
     p.k_first = k_first;
     p.k_stop = split ? (k_split - 1 < klast ? k_split - 1 : klast) : (k_last > 0 ? klast : 0);
+    p.split_cap = (split && d_qrange) ? nq : -1;
     void* args[] = {&p};
     PE_CUDA_TRY(cudaLaunchKernel(fn, dim3((unsigned)grid), dim3(block), args, smem, st));
     if (!split) return PE_OK;
@@ -339,7 +343,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     void* fpart[2] = {find_split_partial_kernel(precision, tpl, kpm), find_split_partial_kernel(PE_PRECISION_F64, tpl, kpm)};
     void* fdraw[2] = {find_split_draw_kernel(precision, tpl, kpm), find_split_draw_kernel(PE_PRECISION_F64, tpl, kpm)};
     int64_t gpart[2], gdraw[2];
-    const int64_t items = S * (int64_t)nch;
+    const int64_t items = nq * (int64_t)nch;
     for (int q = 0; q < npass; ++q) {
         if (!fpart[q] || !fdraw[q]) return PE_ERR_SIZE;
         int per_part = 0, per_draw = 0;
@@ -348,15 +352,17 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
         if ((rc = launch_prepare(fpart[q], block, smem_fixed_bytes_for(kpm, pq), &per_part)) != PE_OK) return rc;
         if ((rc = launch_prepare(fdraw[q], block, sdraw, &per_draw)) != PE_OK) return rc;
         gpart[q] = items < (int64_t)sms * per_part ? items : (int64_t)sms * per_part;
-        gdraw[q] = S < (int64_t)sms * per_draw ? S : (int64_t)sms * per_draw;
+        gdraw[q] = nq < (int64_t)sms * per_draw ? nq : (int64_t)sms * per_draw;
     }
     SplitParams sp;
     sp.c = p;
     sp.nch = nch;
+    sp.nq = nq;
     sp.partial = (double2*)((char*)d_workspace + WS_BYTES);
     sp.flag = (int*)((char*)d_workspace + WS_BYTES + part_bytes);
     void* sargs[] = {&sp};
-    for (int k = (k_split > k_first ? k_split : k_first); k <= klast; ++k) {
+    const int ksplit_last = (nk_max > 0 && nk_max < klast) ? nk_max : klast;
+    for (int k = (k_split > k_first ? k_split : k_first); k <= ksplit_last; ++k) {
         sp.k = k;
         for (int q = 0; q < npass; ++q) {
             sp.pass = q;
@@ -395,6 +401,27 @@ extern "C" int pe_fock_chain_range(int precision, const double* d_acol, const in
                         d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ, occ_stride, d_marg,
                         marg_stride, d_workspace, workspace_bytes, block_threads, tpl, grid_ctas, 0, 1,
                         stream, warp == 1, 1, 0, true, d_qrange, nk_max);
+}
+
+extern "C" size_t pe_range_split_workspace_bytes(int64_t split_slots, int nch) {
+    const size_t q = (size_t)(split_slots < 0 ? 0 : split_slots);
+    return WS_BYTES + q * (size_t)(nch < 1 ? 1 : nch) * MAXN * sizeof(double2) + q * sizeof(int);
+}
+
+extern "C" int pe_fock_chain_range_split(int precision, const double* d_acol, const int64_t* d_inst_off,
+                                         const int32_t* d_inst_m, const int32_t* d_inst_n, int G, int m_max,
+                                         int64_t S, const int64_t* d_dp, const int32_t* d_nk, const int64_t* d_cols,
+                                         int n_stride, const double* d_uniforms, const int64_t* d_seeds,
+                                         const int64_t* d_seed_row, const int64_t* d_rng_off, const int64_t* d_order,
+                                         int64_t* d_rows, int64_t* d_occ, int occ_stride, double* d_marg,
+                                         int marg_stride, void* d_workspace, size_t workspace_bytes,
+                                         int block_threads, int tpl, const int64_t* d_qrange, int nk_max,
+                                         int k_split, int nch, int64_t split_slots, void* stream) {
+    if (!d_qrange || !d_order || !d_nk || nk_max < 1 || k_split < 2 || nch < 1 || split_slots < 1) return PE_ERR_ARG;
+    return chain_launch(precision, d_acol, d_inst_off, d_inst_m, d_inst_n, G, m_max, S, d_dp, d_nk, d_cols, n_stride,
+                        d_uniforms, d_seeds, d_seed_row, d_rng_off, d_order, d_rows, d_occ, occ_stride, d_marg,
+                        marg_stride, d_workspace, workspace_bytes, block_threads, tpl, 0, k_split, nch, stream, false,
+                        1, 0, true, d_qrange, nk_max, split_slots);
 }
 
 extern "C" int pe_fock_chain_warp(int precision, const double* d_acol, const int64_t* d_inst_off,

@@ -78,6 +78,8 @@ struct ChainParams {
     double tau;     // mixed forms: relative guard band of the draw at a step of 20 columns ...
     double tau_log2g;  // ... growing by 2^tau_log2g per column (guard_band)
     int k_stop;     // run steps up to min(nk, k_stop) only (0: all); later steps go to the split kernels
+    int64_t split_cap;  // with qrange: only queue positions below this stop at k_stop (the split kernels' slots);
+                        // later positions run whole here.  -1: every stream stops at k_stop
     int k_first;    // first step to run (1: the whole chain); rows[s][0 .. k_first - 2] are given (a forced
                     // prefix, or the steps of an earlier launch).  A stream with nk < k_first - 1 is skipped.
 };
@@ -330,13 +332,29 @@ static __device__ void prepare_step(SM& sm, const double2* __restrict__ A, int64
     constexpr bool narrow = SM::NK32 == NK;           // the wide layout has no FP32 copy (FP64 only)
     const auto& pl = sm.plan;
     const int tid = threadIdx.x, T = blockDim.x;
-    for (int idx = tid; idx < pl.D * NK; idx += T) {
-        const int kd = idx / NK, j = idx % NK;
-        double2 b = make_double2(0.0, 0.0);
-        if (j < pl.K) b = A[(int64_t)pl.drow[kd] * rs + (int64_t)sm.cols[j] * cs];
-        sm.B[kd][j] = b;
-        if constexpr (narrow)
-            if (mixed && kh == 0) sm.B32[kd][j] = make_float2((float)(2.0 * b.x), (float)(2.0 * b.y));
+    // the gather of B from L2: GB independent loads in flight per thread before any store (one L2 latency
+    // per GB elements instead of one per element)
+    constexpr int GB = 8;
+    const int nel = pl.D * NK;
+    for (int base = tid; base < nel; base += T * GB) {
+        double2 v[GB];
+#pragma unroll
+        for (int g = 0; g < GB; ++g) {
+            const int idx = base + g * T;
+            const bool ok = idx < nel && idx % NK < pl.K;
+            const int kd = ok ? idx / NK : 0, j = ok ? idx % NK : 0;      // in range even when not loaded
+            v[g] = ok ? A[(int64_t)pl.drow[kd] * rs + (int64_t)sm.cols[j] * cs] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int g = 0; g < GB; ++g) {
+            const int idx = base + g * T;
+            if (idx < nel) {
+                const int kd = idx / NK, j = idx % NK;
+                sm.B[kd][j] = v[g];
+                if constexpr (narrow)
+                    if (mixed && kh == 0) sm.B32[kd][j] = make_float2((float)(2.0 * v[g].x), (float)(2.0 * v[g].y));
+            }
+        }
     }
     if (narrow && mixed && kh > 0) {
         __syncthreads();
@@ -1087,7 +1105,7 @@ static __device__ void draw_step(SM& sm, double* __restrict__ wgt, const double2
 
 // ---------------------------------------------------------------------------------------- chain
 template <int TPL, int KPM, int PREC>
-__device__ void chain_one(const ChainParams& p, SmemFor<KPM, PREC>& sm, double* wgt, int64_t s) {
+__device__ void chain_one(const ChainParams& p, SmemFor<KPM, PREC>& sm, double* wgt, int64_t s, bool stop_early) {
     const int tid = threadIdx.x;
     const int64_t g = p.dp[s];
     bool ok = g >= 0 && g < p.G;
@@ -1120,7 +1138,7 @@ __device__ void chain_one(const ChainParams& p, SmemFor<KPM, PREC>& sm, double* 
         __syncthreads();
     }
     const double2* A = p.acol + off;      // (rho, j) at A[j * m + rho]
-    const int kend = (p.k_stop > 0 && p.k_stop < nk) ? p.k_stop : nk;
+    const int kend = (stop_early && p.k_stop > 0 && p.k_stop < nk) ? p.k_stop : nk;
     for (int k = kf; k <= kend; ++k) {
         const int K = k, K1 = k - 1;
         if (K1 == 0) {
@@ -1170,17 +1188,21 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) fock_chain_kernel(ChainParam
     const int tid = threadIdx.x;
     for (;;) {
         if (tid == 0) {
-            sm.cur = queue_stream(p, atomicAdd(p.queue, 1ull));
+            const unsigned long long q = atomicAdd(p.queue, 1ull);
+            sm.cur = queue_stream(p, q);
+            sm.lane0 = (int64_t)q;                  // the ticket, until chain_one resets the field
             sm.bad = 0;
         }
         __syncthreads();
         const int64_t s = sm.cur;
+        const bool stop_early = p.split_cap < 0 || sm.lane0 < p.split_cap;
+        __syncthreads();
         if (s < 0) return;
         if (s >= p.S) {
             if (tid == 0) record_error(p.status, p.detail, s);
             return;
         }
-        chain_one<TPL, KPM, PREC>(p, sm, wgt, s);
+        chain_one<TPL, KPM, PREC>(p, sm, wgt, s, stop_early);
         __syncthreads();
     }
 }
@@ -1194,10 +1216,21 @@ struct SplitParams {
     ChainParams c;
     int k;                  // the step (k columns, k - 1 chosen rows), k >= 2
     int nch;                // CTAs per stream at this step
-    double2* partial;       // [S][nch][MAXN]
-    int* flag;              // [S] mixed forms: 1 when the draw fell in the guard band (redo this step in FP64)
+    int64_t nq;             // slots: streams 0..S-1 (no queue range), or queue positions 0..nq-1 of the range
+    double2* partial;       // [nq][nch][MAXN]
+    int* flag;              // [nq] mixed forms: 1 when the draw fell in the guard band (redo this step in FP64)
     int pass;               // 0: the step; 1: only the flagged streams (FP64 kernels)
 };
+
+// The stream of split slot q: q itself without a queue range; with one, the stream at queue position q of
+// the range order[lo .. hi), or -1 past its end (or for an invalid range, which the persistent kernel
+// records).  Uniform across the CTA.
+static __device__ __forceinline__ int64_t split_stream(const ChainParams& p, int64_t q) {
+    if (!p.qrange) return q;
+    const int64_t lo = p.qrange[0], hi = p.qrange[1];
+    if (lo < 0 || hi > p.S || lo > hi || lo + q >= hi) return -1;
+    return p.order ? p.order[lo + q] : lo + q;
+}
 
 // Stream state of step k from global memory into shared memory; false when the stream has fewer photons
 // than k (nothing to do) or an index is out of range (recorded).  Uniform across the CTA.
@@ -1243,17 +1276,19 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_partial_kernel(SplitPa
     SM& sm = *reinterpret_cast<SM*>(smem_raw);
     const ChainParams& p = sp.c;
     const int tid = threadIdx.x, k = sp.k;
-    for (int64_t item = blockIdx.x; item < p.S * sp.nch; item += gridDim.x) {
-        const int64_t s = item / sp.nch;
+    for (int64_t item = blockIdx.x; item < sp.nq * sp.nch; item += gridDim.x) {
+        const int64_t q = item / sp.nch;
         const int i = (int)(item % sp.nch);
+        const int64_t s = split_stream(p, q);
+        if (s < 0 || s >= p.S) continue;                    // past the range's end: nothing (uniform)
         int m;
         int64_t off;
-        const bool live = (sp.pass == 0 || sp.flag[s] != 0) && load_state(p, sm, s, k, m, off);
+        const bool live = (sp.pass == 0 || sp.flag[q] != 0) && load_state(p, sm, s, k, m, off);
         if (live) {
             if (tid == 0) { sm.lane0 = (int64_t)i * (blockDim.x / TPL); sm.lane_mult = sp.nch; }
             __syncthreads();
             cofactor_step<TPL, KPM, PREC>(sm, p.acol + off, 1, m, k - 1, k);
-            if (tid < k) sp.partial[(s * sp.nch + i) * MAXN + tid] = sm.P[tid];
+            if (tid < k) sp.partial[(q * sp.nch + i) * MAXN + tid] = sm.P[tid];
         }
         __syncthreads();
     }
@@ -1269,15 +1304,17 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_draw_kernel(SplitParam
     double* wgt = reinterpret_cast<double*>(smem_raw + smem_fixed_bytes<KPM, PREC>());
     const ChainParams& p = sp.c;
     const int tid = threadIdx.x, k = sp.k;
-    for (int64_t s = blockIdx.x; s < p.S; s += gridDim.x) {
+    for (int64_t q = blockIdx.x; q < sp.nq; q += gridDim.x) {
+        const int64_t s = split_stream(p, q);
+        if (s < 0 || s >= p.S) continue;                    // past the range's end: nothing (uniform)
         int m;
         int64_t off;
-        if ((sp.pass == 1 && sp.flag[s] == 0) || !load_state(p, sm, s, k, m, off)) { __syncthreads(); continue; }
+        if ((sp.pass == 1 && sp.flag[q] == 0) || !load_state(p, sm, s, k, m, off)) { __syncthreads(); continue; }
         if (tid < k) {
             double xr = 0.0, xi = 0.0;
 #pragma unroll 8
             for (int i = 0; i < sp.nch; ++i) {                 // fixed order; unrolled: loads in flight
-                const double2 v = sp.partial[(s * sp.nch + i) * MAXN + tid];
+                const double2 v = sp.partial[(q * sp.nch + i) * MAXN + tid];
                 xr += v.x;
                 xi += v.y;
             }
@@ -1297,10 +1334,10 @@ __global__ void __launch_bounds__(PE_MAXT, PE_MINB) split_draw_kernel(SplitParam
         draw_step(sm, wgt, A, 1, m, m, k, u, mrow, false);
         if constexpr (PREC != PREC_F64) {
             const bool redo = sm.fmin[0] <= guard_band(p, k);   // guard band: the FP64 pass redoes this step
-            if (tid == 0) sp.flag[s] = redo ? 1 : 0;
+            if (tid == 0) sp.flag[q] = redo ? 1 : 0;
             if (redo) { __syncthreads(); continue; }
         } else {
-            if (sp.pass == 1 && tid == 0) sp.flag[s] = 0;
+            if (sp.pass == 1 && tid == 0) sp.flag[q] = 0;
         }
         if (tid == 0) p.rows[s * p.n_stride + (k - 1)] = sm.rows[k - 1];
         const int nk = p.nk ? p.nk[s] : p.n_stride;

@@ -40,12 +40,27 @@ struct WarpSmem {
 static __device__ void prepare_warp(WarpSmem& sm, const double2* __restrict__ A, int m, bool mixed) {
     const Plan& pl = sm.plan;
     const int lane = threadIdx.x & 31;
-    for (int idx = lane; idx < pl.D * WMAXN; idx += 32) {
-        const int kd = idx / WMAXN, j = idx % WMAXN;
-        double2 b = make_double2(0.0, 0.0);
-        if (j < pl.K) b = A[(int64_t)pl.drow[kd] + (int64_t)sm.cols[j] * m];
-        sm.B[kd][j] = b;
-        if (mixed) sm.B32[kd][j] = make_float2((float)(2.0 * b.x), (float)(2.0 * b.y));
+    // the gather from L2 with GB independent loads in flight per lane before any store
+    constexpr int GB = 8;
+    const int nel = pl.D * WMAXN;
+    for (int base = lane; base < nel; base += 32 * GB) {
+        double2 v[GB];
+#pragma unroll
+        for (int g = 0; g < GB; ++g) {
+            const int idx = base + 32 * g;
+            const bool ok = idx < nel && idx % WMAXN < pl.K;
+            const int kd = ok ? idx / WMAXN : 0, j = ok ? idx % WMAXN : 0;     // in range even when not loaded
+            v[g] = ok ? A[(int64_t)pl.drow[kd] + (int64_t)sm.cols[j] * m] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int g = 0; g < GB; ++g) {
+            const int idx = base + 32 * g;
+            if (idx < nel) {
+                const int kd = idx / WMAXN, j = idx % WMAXN;
+                sm.B[kd][j] = v[g];
+                if (mixed) sm.B32[kd][j] = make_float2((float)(2.0 * v[g].x), (float)(2.0 * v[g].y));
+            }
+        }
     }
     bool bin_in = true, bin_mid = true;             // schedules of radix-2 digits only (distinct rows)
     for (int q = 0; q < pl.nin; ++q) bin_in = bin_in && pl.R[q] == 2;
@@ -190,43 +205,57 @@ __device__ void warp_cofactors(WarpSmem& sm, int K) {
 
 // Marginal, CDF and pick of one step (the rule of cofactors_triton.py:298-308, tot = cw[m - 1]); the
 // 32-mode chunks are scanned twice.  Returns min |cw - u tot| / tot.
-static __device__ double draw_warp(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
-                                   double* __restrict__ marg_row) {
+template <int DRW>
+static __device__ double draw_warp_chunks(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
+                                          double* __restrict__ marg_row) {
     const int lane = threadIdx.x & 31;
     double tot = 0.0;
     for (int pass = 0; pass < 2; ++pass) {
         const double target = u * tot;
         double carry = 0.0, gmin = 1.0e300;
         int cnt = 0;
-        for (int base = 0; base < m; base += 32) {
-            const int rho = base + lane;
-            double w = 0.0;
-            if (rho < m) {
-                double xr = 0.0, xi = 0.0;
-#pragma unroll 4
-                for (int c = 0; c < k; ++c) {                  // unrolled: several loads in flight
-                    const double2 a = A[(int64_t)rho + (int64_t)sm.cols[c] * m];
-                    const double2 p = sm.P[c];
-                    xr = fma(a.x, p.x, xr);
-                    xr = fma(-a.y, p.y, xr);
-                    xi = fma(a.x, p.y, xi);
-                    xi = fma(a.y, p.x, xi);
-                }
-                w = xr * xr + xi * xi;
-            }
-            double x = w;
+        // DRW chunks of 32 modes at a time: DRW independent loads in flight per column and lane (the
+        // amplitudes are the same sums in the same order; the chunks are then scanned one after another)
+        for (int base = 0; base < m; base += 32 * DRW) {
+            double xr[DRW], xi[DRW];
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const double y = __shfl_up_sync(0xffffffffu, x, o);
-                if (lane >= o) x += y;
+            for (int r = 0; r < DRW; ++r) { xr[r] = 0.0; xi[r] = 0.0; }
+#pragma unroll 2
+            for (int c = 0; c < k; ++c) {
+                const int64_t co = (int64_t)sm.cols[c] * m;
+                const double2 p = sm.P[c];
+                double2 a[DRW];
+#pragma unroll
+                for (int r = 0; r < DRW; ++r) {
+                    const int rho = base + 32 * r + lane;
+                    a[r] = rho < m ? A[(int64_t)rho + co] : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int r = 0; r < DRW; ++r) {
+                    xr[r] = fma(a[r].x, p.x, xr[r]);
+                    xr[r] = fma(-a[r].y, p.y, xr[r]);
+                    xi[r] = fma(a[r].x, p.y, xi[r]);
+                    xi[r] = fma(a[r].y, p.x, xi[r]);
+                }
             }
-            const double cw = carry + x;
-            if (pass == 1 && rho < m) {
-                cnt += (cw < target) ? 1 : 0;
-                gmin = fmin(gmin, fabs(cw - target));
-                if (marg_row) marg_row[rho] = w / tot;
+#pragma unroll
+            for (int r = 0; r < DRW; ++r) {
+                const int rho = base + 32 * r + lane;
+                const double w = rho < m ? xr[r] * xr[r] + xi[r] * xi[r] : 0.0;
+                double x = w;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const double y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += y;
+                }
+                const double cw = carry + x;
+                if (pass == 1 && rho < m) {
+                    cnt += (cw < target) ? 1 : 0;
+                    gmin = fmin(gmin, fabs(cw - target));
+                    if (marg_row) marg_row[rho] = w / tot;
+                }
+                carry = __shfl_sync(0xffffffffu, cw, 31);
             }
-            carry = __shfl_sync(0xffffffffu, cw, 31);
         }
         if (pass == 0) {
             tot = carry;
@@ -242,6 +271,13 @@ static __device__ double draw_warp(WarpSmem& sm, const double2* __restrict__ A, 
         }
     }
     return 0.0;
+}
+
+// Four 32-mode chunks at a time when there are many modes (L2 latency hidden by independent loads), one
+// when there are few (four chunks would mostly scan padding: 12-64 modes, 16 % slower).
+static __device__ double draw_warp(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
+                                   double* __restrict__ marg_row) {
+    return m > 96 ? draw_warp_chunks<4>(sm, A, m, k, u, marg_row) : draw_warp_chunks<1>(sm, A, m, k, u, marg_row);
 }
 
 template <int TPL, int KPW, bool MIXED>

@@ -92,6 +92,25 @@ def test_length_tiers_give_the_single_launch_samples(precision):
     assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
 
 
+@pytest.mark.parametrize("precision", ["f64", "mixed"])
+def test_long_chain_split_tier_gives_the_single_launch_samples(precision):
+    """Chains of 25 and 26 photons (a 26-photon circuit at eta = 0.78, 1 600 shots: about a dozen per batch)
+    run in their own tier with their heavy steps split over many CTAs (pe_fock_chain_range_split); the
+    samples equal those of one launch sized to the longest chain, which runs every chain in one CTA."""
+    U = torch.tensor(O.haar_unitary(60, 26), device=DEV)
+    circ = [(U, list(range(26)))]
+    out = []
+    for tiers in (True, False):
+        bs = BatchedSampler(circ, 1600, loss=0.78, precision=precision, seed=9, tune=False, tiers=tiers)
+        if tiers:
+            assert bs.long_split is not None and bs.tiers[0][1] == 2
+            assert int((bs.nk > 24).sum()) >= 0
+        out.append((bs.sample().clone(), bs.sample().clone()))
+        bs.check()
+    n_long = int((bs.nk > 24).sum())
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1]), n_long
+
+
 def test_a_tier_reports_a_chain_longer_than_its_kernel_and_a_bad_range():
     from photonic_engines_b200 import _native as N
     from photonic_engines_b200.clifford.kernels import pack_instances
