@@ -81,6 +81,12 @@ def default_tpl(n: int, precision: str) -> int:
 
 
 NCH_MAX = 512                # CTAs per stream at most
+# split work items (streams x nch) per resident split CTA, at least; more for chains of 24+ photons, whose
+# later steps have fewer live streams and far more terms (measured, FP64 ms: c4 n = 28 m = 784 200 shots
+# 471 -> 379, n = 28 m = 56 256 shots 150 -> 124, n = 26 m = 52 512 shots 84 -> 76; n = 32 m = 64 32 shots
+# 195 -> 204; for n = 20, m = 400, 100 shots the smaller fill stays faster, 2.6 against 3.3)
+SPLIT_FILL = 6
+SPLIT_FILL_LONG = 24
 
 # Chains of at most this many photons run the FP64 kernels when the plain mixed form is asked for: their
 # sweeps are too short for FP32 to pay (n = 6, m = 12, 10 000 shots: mixed 36.3 M against FP64 39.0 M
@@ -107,8 +113,8 @@ def split_plan(heavy_streams: int, n: int, device, block_threads: int = 0, tpl: 
     already fills the GPU several times over.  nch CTAs share every step k >= k_split of a stream.
 
     nch is a power of two (a step's Gray lanes come in powers of two, so any other count leaves lanes idle)
-    with heavy_streams * nch at least six times the split kernel's resident CTAs (`pe_split_slots`), so
-    that the last partial wave costs little; at most 512, and at most what leaves the last four steps split
+    with heavy_streams * nch at least SPLIT_FILL (24 photons and more: SPLIT_FILL_LONG) times the split
+    kernel's resident CTAs (`pe_split_slots`), so that the last partial wave costs little; at most 512, and at most what leaves the last four steps split
     (2^(n-2) / (32 lanes)); of nch and 2 nch the one that fills its waves better (by more than 2 %) wins.  k_split is the first step with enough Gray terms (2^(k-2)) for every
     CTA to run several lanes.  The reference's single-sample path sizes a fixed lane grid instead
     (photonic_engines/clifford/single.py:22-82)."""
@@ -130,7 +136,8 @@ def split_plan(heavy_streams: int, n: int, device, block_threads: int = 0, tpl: 
     # at most enough CTAs for the last four steps to be split (short chains: earlier steps stay whole)
     cap = max(1, min(NCH_MAX, (1 << (n - 2)) // (32 * lanes)))
     nch = 1
-    while nch < cap and heavy_streams * nch < 6 * slots:
+    fill = SPLIT_FILL_LONG if n >= 24 else SPLIT_FILL
+    while nch < cap and heavy_streams * nch < fill * slots:
         nch *= 2
     if 2 * nch <= cap and fill(2 * nch) > fill(nch) + 0.02:
         nch *= 2
