@@ -136,8 +136,8 @@ def split_plan(heavy_streams: int, n: int, device, block_threads: int = 0, tpl: 
     # at most enough CTAs for the last four steps to be split (short chains: earlier steps stay whole)
     cap = max(1, min(NCH_MAX, (1 << (n - 2)) // (32 * lanes)))
     nch = 1
-    fill = SPLIT_FILL_LONG if n >= 24 else SPLIT_FILL
-    while nch < cap and heavy_streams * nch < fill * slots:
+    waves = SPLIT_FILL_LONG if n >= 24 else SPLIT_FILL
+    while nch < cap and heavy_streams * nch < waves * slots:
         nch *= 2
     if 2 * nch <= cap and fill(2 * nch) > fill(nch) + 0.02:
         nch *= 2

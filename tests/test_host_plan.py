@@ -93,3 +93,27 @@ def test_loss_only_plan_in_tensor_ops_is_the_general_plan(n, m, S, eta, in_modes
     for f in ("dp", "cols", "nk", "seeds", "seed_row", "rng_off", "out_row", "order", "single_ids", "single_rows"):
         x, y = getattr(a, f), getattr(b, f)
         assert (x is None and y is None) or torch.equal(x, y), f
+
+
+@pytest.mark.parametrize(("heavy", "n", "slots", "expect"), [
+    (200, 28, 296, (17, 64)),       # 200 streams of 28 photons: 24 waves of the resident CTAs
+    (2000, 20, 296, None),          # many streams: one CTA each already fills the GPU
+    (1, 20, 296, (17, 64)),         # one stream: as many CTAs as the cap (2^18 terms / 32 lanes) allows
+    (3, 6, 296, None),              # short chains are never split
+])
+def test_split_plan_sizes_the_ctas_per_stream_from_the_resident_slots(monkeypatch, heavy, n, slots, expect):
+    """The split planner on the CPU, with the resident-CTA count the library would report stubbed: nch is a
+    power of two filling SPLIT_FILL (SPLIT_FILL_LONG from 24 photons) waves, capped; k_split leaves every
+    split step several Gray lanes per CTA."""
+    from photonic_engines_b200.clifford import kernels as K
+    monkeypatch.setattr(K, "_split_slots", lambda *a: slots)
+    plan = K.split_plan(heavy, n, "cuda:0", 128, 1, "f64")
+    if expect is None:
+        assert plan is None
+        return
+    k, nch = plan
+    assert nch & (nch - 1) == 0 and nch <= K.NCH_MAX
+    waves = K.SPLIT_FILL_LONG if n >= 24 else K.SPLIT_FILL
+    assert heavy * nch >= waves * slots or nch == min(K.NCH_MAX, (1 << (n - 2)) // (32 * 128))
+    assert (1 << (k - 2)) >= 4 * nch * 128 and (1 << (k - 3)) < 4 * nch * 128
+    assert (k, nch) == expect
