@@ -147,6 +147,71 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def _reference_fock_sample():
+    """The reference's public fock_sample from its offline install in baseline/_ref, or (None, why)."""
+    ref = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref, "photonic_engines")):
+        return None, "baseline/_ref holds no install of the reference"
+    try:
+        import triton  # noqa: F401
+    except ImportError:
+        return None, "triton is not importable (the reference's GPU engine is Triton)"
+    sys.path.insert(0, ref)
+    try:
+        import photonic_engines.clifford as rc
+    finally:
+        sys.path.remove(ref)
+    return rc.fock_sample, None
+
+
+def public_call_leg(circuits, shots, loss=None, indist=None, reps: int = 1, ours: bool = True) -> dict:
+    """One public sampling call per circuit, through the reference's own GPU engine (its fock_sample with its
+    default Triton backend, unmodified, from baseline/_ref) and, with `ours`, through this library's
+    fock_sample (FP64, the drop-in), from equal CUDA generator seeds on this GPU.  Per engine: samples/s over
+    `reps` timed rounds (CUDA events, after one untimed round that also builds the reference's Triton
+    kernels); and how many occupation rows of the last round agree between the two."""
+    import torch
+    ref_fn, why = _reference_fock_sample()
+    if ref_fn is None:
+        return {"unavailable": why}
+    engines = [("reference", ref_fn)]
+    if ours:
+        from photonic_engines_b200.clifford import fock_sample
+        engines.append(("fock_sample", fock_sample))
+    total = shots * len(circuits)
+
+    def run(fn, seed):
+        outs = []
+        for i, (U, modes) in enumerate(circuits):
+            kw = {}
+            if loss is not None:
+                kw["loss"] = loss[i] if isinstance(loss, list) else loss
+            if indist is not None:
+                kw["indist"] = indist
+            outs.append(fn(U, modes, shots, generator=torch.Generator(device=U.device).manual_seed(seed + i), **kw))
+        return outs
+
+    res, last = {}, {}
+    for name, fn in engines:
+        run(fn, 1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for r in range(reps):
+            last[name] = run(fn, 7 + 100000 * r)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        res[name] = {"value": total / (ms * 1e-3), "unit": "samples/s", "ms_per_call_round": ms}
+    res["reference"]["engine"] = "reference photonic_engines.clifford.fock_sample, backend triton (its default)"
+    if ours:
+        same = sum(int((a.cpu() == b.cpu()).all(dim=1).sum()) for a, b in zip(last["reference"], last["fock_sample"]))
+        res["identical_rows"] = same
+        res["rows"] = total
+    res["calls_per_round"] = len(circuits)
+    return res
+
+
 def reference_torch_sampler(shots: int = 1) -> dict:
     """The reference's own CPU sampler for this path, unmodified, from its offline install in baseline/_ref:
     variants.fock_sample_reference (photonic_engines/clifford/variants.py:218-241, pure torch, FP64) on `shots`
@@ -301,7 +366,13 @@ def run_b200(args):
 
     configs = None
     if rank == 0 and ws == 1 and not args.no_configs:
-        configs = {name: config_result(name, min(args.steps, 3), 3) for name in ("c3", "c4", "c5")}
+        configs = {name: config_result(name, min(args.steps, 3), 3, not args.no_reference_gpu)
+                   for name in ("c3", "c4", "c5")}
+
+    # the same public call through the reference's own GPU engine on this GPU, and row-for-row agreement
+    ref_gpu = None
+    if rank == 0 and ws == 1 and not args.no_reference_gpu:
+        ref_gpu = public_call_leg([(U, in_modes)], SHOTS, reps=3)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -355,6 +426,7 @@ def run_b200(args):
             "clocks": res[head]["clocks"],
             "gpu_launches": args.steps,
             "configs": configs,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -423,7 +495,7 @@ def hbm_peak() -> tuple[float, str]:
         return 6650.0, "of fallback (6.65 TB/s)"
 
 
-def config_result(name: str, steps: int, warmup: int) -> dict:
+def config_result(name: str, steps: int, warmup: int, reference_gpu: bool = True) -> dict:
     """One configuration run through the batched sampler (one persistent launch per batch, CUDA-graph
     replay) in every form: samples/s, roofline of the chain kernel, end to end with the occupations copied
     to the host, occupations equal to the FP64 form's, and the marginal error of the FP32 forms against
@@ -515,14 +587,17 @@ def config_result(name: str, steps: int, warmup: int) -> dict:
                               over_fp64=out[precision]["value"] / out["f64"]["value"])
     out["f64"].update(max_marginal_rel_err=0.0, meets_bound=True)
     head = max((f for f in FORMS if out[f]["meets_bound"]), key=lambda f: out[f]["value"])
+    # the configuration's public calls (one fock_sample per circuit) through the reference's own GPU engine
+    # and through this library's drop-in fock_sample, with row-for-row agreement
+    ref_gpu = public_call_leg(circuits, shots, loss, indist) if reference_gpu else None
     return {"config": name, "workload": desc, "metric": "samples/s", "unit": "samples/s",
             "value": out[head]["value"], "headline_form": head, "forms": out, "steps": steps, "warmup": warmup,
-            "data": "synthetic"}
+            "data": "synthetic", "reference_gpu": ref_gpu}
 
 
 def run_config(args):
     """`--config c1|c3|c4|c5`: one JSON line for that configuration (config_result)."""
-    line = config_result(args.config, args.steps, args.warmup)
+    line = config_result(args.config, args.steps, args.warmup, not args.no_reference_gpu)
     line.update(n_gpus=1)
     print(json.dumps(line), flush=True)
 
@@ -774,6 +849,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
     ap.add_argument("--ref-shots", type=int, default=0, help="chains per CPU sample (0: scaled to the cores)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU engine (baseline/_ref, Triton) on the same calls")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the c3 / c4 / c5 results the default line carries under 'configs'")
     ap.add_argument("--config", choices=("c1", "c2", "c3", "c4", "c5", "emitter", "single", "adaptive", "published"),

@@ -160,6 +160,112 @@ def use_warp_form(S: int, n: int, device) -> bool:
     return n <= 12 or S >= 64 * torch.cuda.get_device_properties(device).multi_processor_count
 
 
+# Length tiers of a ragged launch (lossy or partially distinguishable shots): the photon counts at which the
+# longest-first queue is cut, so that every chain runs in the smallest kernel variant that holds it, and the
+# count above which the few longest chains have their heavy steps split over several CTAs (one 26-photon
+# survivor at m = 900 otherwise holds one CTA for longer than all the other chains of 10 000 shots take).
+TIER_CUTS = (20, 16)
+LONG_SPLIT_ABOVE = 24
+
+
+def tier_plan(counts: dict, n_stride: int, precision: str, device) -> list:
+    """The tiers of a ragged launch whose chains are queued longest first: counts {photons: chains} ->
+    [(lo, hi, nk_max, mode, split)] over queue positions [lo, hi), chains of at most nk_max photons; mode 0
+    one CTA per chain, 1 one warp per chain (the last tier, up to 16 photons, FP64 and mixed forms), 2 one
+    CTA per chain with steps k_split.. spread over nch CTAs (split = (k_split, nch), the chains above
+    LONG_SPLIT_ABOVE photons when they are too few to fill the GPU).  Empty counts give no tier."""
+    bounds = [n_stride] + ([LONG_SPLIT_ABOVE] if n_stride > LONG_SPLIT_ABOVE else [])
+    bounds += [c for c in TIER_CUTS if c < bounds[-1]] + [0]
+    tiers, pos = [], 0
+    for i in range(len(bounds) - 1):
+        ks = [k for k, c in counts.items() if bounds[i + 1] < k <= bounds[i] and c > 0]
+        if not ks:
+            continue
+        cnt, nk_max = sum(counts[k] for k in ks), max(ks)
+        mode, split = 0, None
+        if bounds[i + 1] == LONG_SPLIT_ABOVE:
+            split = split_plan(cnt, nk_max, device, DEFAULT_BLOCK, default_tpl(nk_max, precision), precision)
+            mode = 2 if split else 0
+        elif bounds[i + 1] == 0 and precision != "compensated" and use_warp_form(cnt, nk_max, device):
+            mode = 1
+        tiers.append((pos, pos + cnt, nk_max, mode, split))
+        pos += cnt
+    return tiers
+
+
+_SIDE_STREAMS: dict = {}
+
+
+def _side_streams(dev, count: int) -> list:
+    """Side streams of a device for concurrent tiers (made once, reused)."""
+    key = dev.index if dev.index is not None else torch.cuda.current_device()
+    have = _SIDE_STREAMS.setdefault(key, [])
+    while len(have) < count:
+        have.append(torch.cuda.Stream(dev))
+    return have[:count]
+
+
+def chain_tiers(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst_n: torch.Tensor, dp, cols, nk,
+                order, tiers, *, m_max: int, seeds, seed_row=None, rng_off=None, precision: str = "f64",
+                check_status: bool = True) -> torch.Tensor:
+    """Ragged chains (nk [C] photons, order [C] queue of chains longest first) in the length tiers of
+    `tier_plan`, one launch per tier (pe_fock_chain_range / pe_fock_chain_range_split), the tiers on
+    concurrent streams joined back into the current one.  Philox draws from seeds only.  Returns the
+    ordered rows [C, n_stride] (entries past nk[c] untouched, zero)."""
+    N.require_cuda(acol, "acol")
+    dev = acol.device
+    L = N.load()
+    if precision not in N.PRECISIONS:
+        raise ValueError(f"unknown precision {precision!r}: 'f64', 'mixed' or 'compensated'")
+    dp, cols, order_t = _i64(dp, dev), _i64(cols, dev), _i64(order, dev)
+    C, n_stride = cols.shape
+    N.check_photons(n_stride, precision)
+    nk_t = torch.as_tensor(nk, dtype=torch.int32, device=dev).contiguous()
+    seeds_t = _i64(seeds, dev)
+    if seeds_t.dim() == 1:
+        seeds_t = seeds_t[None]
+    if seeds_t.shape[-1] != n_stride:
+        seeds_t = torch.nn.functional.pad(seeds_t, (0, n_stride - seeds_t.shape[-1])).contiguous()
+    seed_row_t, rng_off_t = _i64(seed_row, dev), _i64(rng_off, dev)
+    _seed_rows(seeds_t, seed_row_t)
+    if not tiers or tiers[-1][1] != C or any(a[1] != b[0] for a, b in zip(tiers, tiers[1:])) or tiers[0][0] != 0:
+        raise ValueError("tiers: consecutive queue ranges covering every chain expected")
+    rows = torch.zeros(C, n_stride, dtype=torch.int64, device=dev)
+    a = acol if acol.dtype == torch.float64 else torch.view_as_real(acol.contiguous())
+    # every buffer a tier reads is made on the current stream before the side streams wait on it
+    qr = torch.tensor([[lo, hi] for lo, hi, *_ in tiers], dtype=torch.int64, device=dev)
+    wss = []
+    for lo, hi, nk_max, mode, split in tiers:
+        nb = L.pe_range_split_workspace_bytes(hi - lo, split[1]) if mode == 2 else L.pe_chain_workspace_bytes(C)
+        wss.append(torch.zeros(int(nb), dtype=torch.uint8, device=dev))
+    cur = torch.cuda.current_stream(dev)
+    side = _side_streams(dev, len(tiers) - 1)
+    for s_ in side:
+        s_.wait_stream(cur)
+    for i, (lo, hi, nk_max, mode, split) in enumerate(tiers):
+        st = (cur if i == 0 else side[i - 1]).cuda_stream
+        prec = effective_precision(precision, nk_max)
+        common = (N.PRECISIONS[prec], N.ptr(a), N.ptr(inst_off), N.ptr(inst_m), N.ptr(inst_n), int(inst_off.shape[0]),
+                  int(m_max), int(C), N.ptr(dp), N.ptr(nk_t), N.ptr(cols), int(n_stride), None, N.ptr(seeds_t),
+                  N.ptr(seed_row_t), N.ptr(rng_off_t), N.ptr(order_t), N.ptr(rows), None, int(m_max), None,
+                  int(m_max), N.ptr(wss[i]), int(wss[i].numel()))
+        if mode == 2:
+            rc = L.pe_fock_chain_range_split(*common, DEFAULT_BLOCK, default_tpl(nk_max, prec), N.ptr(qr[i]), int(nk_max),
+                                             int(split[0]), int(split[1]), int(hi - lo), st)
+            N.check(rc, "pe_fock_chain_range_split")
+        else:
+            rc = L.pe_fock_chain_range(*common, 0, 0, 0, N.ptr(qr[i]), int(nk_max), int(mode), st)
+            N.check(rc, "pe_fock_chain_range")
+    for s_ in side:
+        cur.wait_stream(s_)
+    if check_status:
+        for ws in wss:
+            st_, det = N.read_status(ws)
+            if st_ != 0:
+                raise N.NativeError(f"pe_fock_chain_range: device-side index error at stream {det} (status {st_})")
+    return rows
+
+
 def chain(acol: torch.Tensor, inst_off: torch.Tensor, inst_m: torch.Tensor, inst_n: torch.Tensor, dp, cols, *,
           m_max: int | None = None, nk=None, uniforms=None, seeds=None, seed_row=None, rng_off=None, order=None,
           want_occ: bool = True, occ_stride: int | None = None, want_marg: bool = False, precision: str = "f64",

@@ -12,7 +12,10 @@ argument meaning, stream layout (row s = b * shots + shot), error behaviour and 
     photons are routed classically on the host.
 
 What differs is the execution: every chain of every pass runs in ONE launch of the persistent chain kernel
-(no per-step launches, no per-pass copies of U's columns, no host synchronisation inside the chain).
+(no per-step launches, no per-pass copies of U's columns, no host synchronisation inside the chain); a
+ragged call (loss, partial distinguishability) runs one launch per length tier instead, on concurrent
+streams, each tier in the smallest kernel variant that holds its chains and its few longest chains with
+their heavy steps split over several CTAs (kernels.tier_plan).
 """
 from __future__ import annotations
 
@@ -23,7 +26,7 @@ import torch
 
 from .. import _native as N
 from ..imperfections import as_model, draw_fates, group_fates, route_lone_photons
-from .kernels import chain, chain_adaptive, default_tpl, pack_instances, split_plan
+from .kernels import chain, chain_adaptive, chain_tiers, default_tpl, pack_instances, split_plan, tier_plan
 from .prefix import prefix_order
 
 BACKENDS = ("b200", "triton", "cuda", "exq")
@@ -104,8 +107,8 @@ def fock_sample(U, in_modes, shots, generator=None, algo="auto", multi_min_k1=10
     marginals and CDF; ~1e-5 marginals at 20 photons; chains of at most 8 photons run the FP64 kernels, which
     are faster there) or "compensated" (double-float FP32 Gray blocks: FP64-level marginals); every form
     returns the FP64 form's samples.  uniforms: optional float64 [S, n] per-step uniforms replacing the Philox draws
-    (lossless only).  stats: receives "passes" = [(k, streams, seconds)] — all passes run in one launch, so
-    every entry carries that launch's time — and "fused_seconds".
+    (lossless only).  stats: receives "passes" = [(k, streams, seconds)] — all passes run in one launch (one
+    per length tier when ragged), so every entry carries the launches' time — and "fused_seconds".
     prefix (adaptive sampling, lossless only): the output modes the FIRST c photons of every chain are forced
     onto — a list of c modes shared by all circuits, or an int tensor [B, c]; the column set of those c steps
     is drawn from its posterior |per(A[prefix, T])|^2 (`prefix.prefix_columns_many`) and the chain runs steps
@@ -183,14 +186,25 @@ def fock_sample(U, in_modes, shots, generator=None, algo="auto", multi_min_k1=10
     direct = plan.out_row is None
     if plan.C > 0:
         u = None if uniforms is None else torch.as_tensor(uniforms, dtype=torch.float64, device=dev)
-        heavy = plan.C if plan.nk is None else int((plan.nk >= 8).sum())
-        rows, occ_k, _ = chain(acol, inst_off, inst_m, inst_n, plan.dp, plan.cols, m_max=m, nk=plan.nk, uniforms=u,
-                               seeds=plan.seeds, seed_row=plan.seed_row, rng_off=plan.rng_off, order=plan.order,
-                               want_occ=direct, precision=precision, block_threads=block_threads, tpl=tpl,
-                               split=split_plan(heavy, n, dev, block_threads,
-                                                tpl or default_tpl(n, precision), precision))
-        if direct:
-            occ = occ_k
+        tiers = []
+        if plan.nk is not None and not direct and u is None and not block_threads and not tpl:
+            counts: dict = {}
+            for k, cnt in plan.passes:
+                counts[k] = counts.get(k, 0) + cnt
+            tiers = tier_plan(counts, n, precision, dev)
+        if len(tiers) > 1 or (tiers and tiers[0][3] == 2):     # ragged: every length in its own tier
+            rows = chain_tiers(acol, inst_off, inst_m, inst_n, plan.dp, plan.cols, plan.nk, plan.order, tiers,
+                               m_max=m, seeds=plan.seeds, seed_row=plan.seed_row, rng_off=plan.rng_off,
+                               precision=precision)
+        else:
+            heavy = plan.C if plan.nk is None else int((plan.nk >= 8).sum())
+            rows, occ_k, _ = chain(acol, inst_off, inst_m, inst_n, plan.dp, plan.cols, m_max=m, nk=plan.nk, uniforms=u,
+                                   seeds=plan.seeds, seed_row=plan.seed_row, rng_off=plan.rng_off, order=plan.order,
+                                   want_occ=direct, precision=precision, block_threads=block_threads, tpl=tpl,
+                                   split=split_plan(heavy, n, dev, block_threads,
+                                                    tpl or default_tpl(n, precision), precision))
+            if direct:
+                occ = occ_k
     if stats is not None:
         torch.cuda.synchronize(dev)
         stats["fused_seconds"] = _time.perf_counter() - t0
