@@ -793,7 +793,8 @@ def run_published(args):
     """`--config published`: the workloads of the reference's published H100 numbers, run here through the
     public fock_sample (FP64, photons in modes 0..n-1, seeded Haar U, CUDA generator), one line with this
     GPU's figure, the published one and their ratio (> 1: faster here), frontier rows up to 40 photons
-    included."""
+    included; beside them the reference's own engine (its fock_sample, Triton backend, from baseline/_ref)
+    on this GPU for the same call, and how many of its occupation rows ours reproduces."""
     import numpy as np
     import torch
 
@@ -802,6 +803,7 @@ def run_published(args):
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
+    ref_fn, ref_why = (None, "skipped (--no-reference-gpu)") if args.no_reference_gpu else _reference_fock_sample()
     rows_out = []
     for label, n, m, shots, loss, pub, unit, src in PUBLISHED:
         g = torch.Generator().manual_seed(1000 + n + m)
@@ -832,12 +834,34 @@ def run_published(args):
             add = chain_work(res["rows"].cpu().numpy(), m)["addends"] / sig.shape[0]
             row.update(addends_per_sample=add, g_addends_per_s=add / dt / 1e9,
                        published_g_addends_per_s=PUBLISHED_ADDENDS[n] / 1e9)
+        if ref_fn is None:
+            row["reference_b200"] = {"unavailable": ref_why}
+        else:
+            # the reference's own engine (Triton backend) on this GPU, the same call; shots cut so that one
+            # call stays near 20 s at four times the published H100 time per sample
+            pub_s = {"s/sample": pub, "ms/sample": pub * 1e-3, "samples/s": 1.0 / pub}[unit]
+            ref_shots = shots if 4 * pub_s * shots <= 20 else max(1, int(20 / (4 * pub_s)))
+            ref_fn(U, list(range(n)), 1, generator=torch.Generator(device=dev).manual_seed(3), **kw)  # builds kernels
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            a = ref_fn(U, list(range(n)), ref_shots, generator=torch.Generator(device=dev).manual_seed(11), **kw)
+            torch.cuda.synchronize()
+            dt_ref = (time.perf_counter() - t0) / ref_shots
+            b = fock_sample(U, list(range(n)), ref_shots, generator=torch.Generator(device=dev).manual_seed(11), **kw)
+            same = int((a.cpu() == b.cpu()).all(dim=1).sum())
+            row["reference_b200"] = {"value": {"s/sample": dt_ref, "ms/sample": dt_ref * 1e3, "samples/s": 1.0 / dt_ref}[unit],
+                                     "unit": unit, "shots": ref_shots, "identical_rows": same,
+                                     "engine": "reference photonic_engines.clifford.fock_sample, backend triton"}
+            row["speedup_vs_reference_b200"] = dt_ref / dt
         rows_out.append(row)
         print(json.dumps(row), file=sys.stderr, flush=True)
     line = {"config": "published", "metric": "speed-up over the reference's published H100 numbers (same workloads)",
             "unit": "x", "value": float(np.exp(np.mean([np.log(r_["speedup_vs_h100"]) for r_ in rows_out]))),
             "higher_is_better": True, "dtype": "f64", "data": "synthetic", "n_gpus": 1, "rows": rows_out,
             "note": "geometric mean of the per-row ratios"}
+    on_b200 = [r_["speedup_vs_reference_b200"] for r_ in rows_out if "speedup_vs_reference_b200" in r_]
+    if on_b200:
+        line["speedup_vs_reference_b200_geomean"] = float(np.exp(np.mean(np.log(on_b200))))
     print(json.dumps(line), flush=True)
 
 
