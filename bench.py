@@ -164,7 +164,8 @@ def _reference_fock_sample():
     return rc.fock_sample, None
 
 
-def public_call_leg(circuits, shots, loss=None, indist=None, reps: int = 1, ours: bool = True) -> dict:
+def public_call_leg(circuits, shots, loss=None, indist=None, reps: int = 1, ours: bool = True,
+                    extra: dict | None = None) -> dict:
     """One public sampling call per circuit, through the reference's own GPU engine (its fock_sample with its
     default Triton backend, unmodified, from baseline/_ref) and, with `ours`, through this library's
     fock_sample (FP64, the drop-in), from equal CUDA generator seeds on this GPU.  Per engine: samples/s over
@@ -188,6 +189,7 @@ def public_call_leg(circuits, shots, loss=None, indist=None, reps: int = 1, ours
                 kw["loss"] = loss[i] if isinstance(loss, list) else loss
             if indist is not None:
                 kw["indist"] = indist
+            kw.update(extra or {})
             outs.append(fn(U, modes, shots, generator=torch.Generator(device=U.device).manual_seed(seed + i), **kw))
         return outs
 
@@ -205,9 +207,17 @@ def public_call_leg(circuits, shots, loss=None, indist=None, reps: int = 1, ours
         res[name] = {"value": total / (ms * 1e-3), "unit": "samples/s", "ms_per_call_round": ms}
     res["reference"]["engine"] = "reference photonic_engines.clifford.fock_sample, backend triton (its default)"
     if ours:
-        same = sum(int((a.cpu() == b.cpu()).all(dim=1).sum()) for a, b in zip(last["reference"], last["fock_sample"]))
+        same, rows = 0, 0
+        for a, b in zip(last["reference"], last["fock_sample"]):
+            if isinstance(a, tuple):                 # keep_ids: (occupations, surviving stream ids)
+                if not torch.equal(a[1].cpu(), b[1].cpu()):
+                    rows += a[0].shape[0]
+                    continue
+                a, b = a[0], b[0]
+            same += int((a.cpu() == b.cpu()).all(dim=1).sum()) if a.shape == b.shape else 0
+            rows += a.shape[0]
         res["identical_rows"] = same
-        res["rows"] = total
+        res["rows"] = rows
     res["calls_per_round"] = len(circuits)
     return res
 
@@ -697,8 +707,45 @@ def run_emitter(args):
                     "d2h_bytes_per_step": shots * m * 8},
             "cpu_baseline": {"value": cpu, "unit": "samples/s", "cores": torch.get_num_threads(), "kind": "port",
                              "sample": f"{nb} streams, host pure terms + numpy matrix-cofactor sums per step"},
-            "clocks": clk.summary()}
+            "clocks": clk.summary(),
+            "reference_gpu": None if args.no_reference_gpu else emitter_reference_leg(st, n, m, shots, U, args.steps)}
     print(json.dumps(line), flush=True)
+
+
+def emitter_reference_leg(st, n: int, m: int, shots: int, U, steps: int) -> dict:
+    """The same emitter workload through the reference's own emitter_sample (its default Triton backend,
+    unmodified, from baseline/_ref) on this GPU: samples/s over `steps` calls after one untimed call, and how
+    many occupation rows of the last call ours reproduces from the same generator seed."""
+    import math
+
+    import torch
+
+    from photonic_engines_b200.clifford import emitter_sample
+    ref = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref, "photonic_engines")):
+        return {"unavailable": "baseline/_ref holds no install of the reference"}
+    sys.path.insert(0, ref)
+    try:
+        import photonic_engines.clifford as rc
+        from photonic_engines.states import EmitterMPS, spin_gate
+    finally:
+        sys.path.remove(ref)
+    rst = EmitterMPS.caterpillar(n, [spin_gate(math.pi / 2, 0)] * n, m=m)
+    try:
+        rc.emitter_sample(rst, U, shots, generator=torch.Generator().manual_seed(100))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for i in range(steps):
+            a = rc.emitter_sample(rst, U, shots, generator=torch.Generator().manual_seed(i))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    except Exception as e:                      # the reference's own code refusing this input or device
+        return {"unavailable": f"{type(e).__name__}: {str(e)[:200]}"}
+    b = emitter_sample(st, U, shots, generator=torch.Generator().manual_seed(steps - 1))
+    same = int((a.cpu() == b.cpu()).all(dim=1).sum()) if a.shape == b.shape else 0
+    return {"value": steps * shots / dt, "unit": "samples/s", "ms_per_call": dt / steps * 1e3,
+            "identical_rows": same, "rows": int(a.shape[0]),
+            "engine": "reference photonic_engines.clifford.emitter_sample, backend triton (its default)"}
 
 
 def run_latency_and_adaptive(args):
@@ -746,16 +793,24 @@ def run_latency_and_adaptive(args):
             out[precision] = {"chains_per_s": args.steps * shots / dt, "survivors_per_s": kept / dt,
                               "survival": kept / (args.steps * shots), "ms_per_step": dt / args.steps * 1e3,
                               "clocks": clk.summary()}
+    # the same calls through the reference's own engine (Triton backend) on this GPU, beside ours in FP64
+    ref_gpu = None
+    if not args.no_reference_gpu:
+        if args.config == "single":
+            ref_gpu = public_call_leg([(U, in_modes)], 1, reps=args.steps)
+        else:
+            ref_gpu = public_call_leg([(U, in_modes)], SHOTS, reps=max(1, args.steps // 2),
+                                      extra={"prefix": [0, 1], "avoid": [0, 1], "keep_ids": True})
     if args.config == "single":
         line = {"config": "single", "workload": WORKLOAD.replace("2000 shots/step", "1 shot per call"),
                 "metric": "ms per sample (latency)", "unit": "ms", "value": out["f64"]["ms_per_sample"],
                 "higher_is_better": False, "fp64": out["f64"], "mixed": out["mixed"], "n_gpus": 1,
-                "steps": args.steps, "warmup": args.warmup, "data": "synthetic"}
+                "steps": args.steps, "warmup": args.warmup, "data": "synthetic", "reference_gpu": ref_gpu}
     else:
         line = {"config": "adaptive", "workload": WORKLOAD + ", prefix (0, 1), avoid (0, 1)",
                 "metric": "surviving samples/s", "unit": "samples/s", "value": out["mixed"]["survivors_per_s"],
                 "higher_is_better": True, "fp64": out["f64"], "mixed": out["mixed"], "n_gpus": 1,
-                "steps": args.steps, "warmup": args.warmup, "data": "synthetic"}
+                "steps": args.steps, "warmup": args.warmup, "data": "synthetic", "reference_gpu": ref_gpu}
     print(json.dumps(line), flush=True)
 
 
