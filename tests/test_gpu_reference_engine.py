@@ -101,3 +101,44 @@ def test_prefix_and_avoid(ref):
     a, ia = ref(U, list(range(10)), 400, generator=_gen(19), prefix=[0, 1], avoid=[2, 3], keep_ids=True)
     b, ib = fock_sample(U, list(range(10)), 400, generator=_gen(19), prefix=[0, 1], avoid=[2, 3], keep_ids=True)
     assert torch.equal(ia.cpu(), ib.cpu()) and torch.equal(a.cpu(), b.cpu())
+
+
+def test_single_sample_and_short_chains(ref):
+    """One shot per call (the split latency path) and the n = 6, m = 12 workload (warp form)."""
+    U = torch.tensor(O.haar_unitary(400, 1002), device=DEV)
+    for seed in (21, 22, 23):
+        _same(ref, U, list(range(20)), 1, seed)
+    U12 = torch.tensor(O.haar_unitary(12, 1001), device=DEV)
+    _same(ref, U12, list(range(6)), 10000, 24)
+
+
+@pytest.fixture(scope="module")
+def ref_emitter():
+    if not os.path.isdir(os.path.join(REF, "photonic_engines")):
+        pytest.skip("the reference is not installed in baseline/_ref")
+    pytest.importorskip("triton")
+    sys.path.insert(0, REF)
+    try:
+        import photonic_engines.clifford as rc
+        from photonic_engines.states import EmitterMPS, spin_gate
+    finally:
+        sys.path.remove(REF)
+    return rc.emitter_sample, EmitterMPS, spin_gate
+
+
+@pytest.mark.parametrize("kw", [{}, {"loss": 0.8}, {"loss": 0.8, "unravel": False}, {"indist": 0.9}])
+def test_emitter_caterpillar(ref_emitter, kw):
+    """The linear cluster state of 8 photons in 16 modes, emitter traced, through both emitter_sample calls
+    with equal CPU generator seeds (the generator the reference's emitter path draws its host choices from)."""
+    import math
+
+    from photonic_engines_b200.clifford import emitter_sample
+    from photonic_engines_b200.states import caterpillar, spin_gate
+    ref_fn, EmitterMPS, ref_gate = ref_emitter
+    n, m = 8, 16
+    U = torch.tensor(O.haar_unitary(m, 88), device=DEV)
+    rst = EmitterMPS.caterpillar(n, [ref_gate(math.pi / 2, 0)] * n, m=m)
+    st = caterpillar(n, [spin_gate(math.pi / 2, 0)] * n, m=m)
+    a = ref_fn(rst, U, 256, generator=torch.Generator().manual_seed(31), **kw)
+    b = emitter_sample(st, U, 256, generator=torch.Generator().manual_seed(31), **kw)
+    assert torch.equal(a.cpu(), b.cpu())
