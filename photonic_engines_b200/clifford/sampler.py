@@ -380,31 +380,50 @@ def _plan_loss_only(U, in_modes, S, dp_all, generator, gen, loss, max_streams) -
     rank = torch.full((n + 1,), len(ks), dtype=torch.int64)
     for r_, k in enumerate(ks):
         rank[k] = r_
-    ch_dp, ch_cols, ch_nk, ch_row, ch_off, ch_out, all_seeds, passes = [], [], [], [], [], [], [], []
-    n_rows = 0
+    passes, tabs = [], []
     if ks:
         key = rank[kg[inv]] * G + inv                                    # pass, then group; streams stable
         key[kg[inv] < 2] = len(ks) * G + G                               # not in a pass
         order_s = torch.sort(key, stable=True).indices
         skey = key[order_s]
-        im = torch.as_tensor([int(j) for j in in_modes], dtype=torch.int64)
+        # the host side of every pass (no generator use): its streams in order and each stream's photons
         for r_, k in enumerate(ks):
             sel = order_s[(skey >= r_ * G) & (skey < (r_ + 1) * G)]     # streams of this pass, in order
-            gsel = inv[sel]
-            groups_k, gidx = torch.unique_consecutive(gsel, return_inverse=True)
-            subs = torch.nonzero(kept[groups_k])[:, 1].reshape(-1, k).to(dev)        # [groups, k] photon ids
-            sig, seeds, chunk, off = _pass_draws(int(sel.shape[0]), k, generator, dev, max_streams)
-            ch_dp.append(dp_all[sel.to(dev)])
-            ch_cols.append(torch.nn.functional.pad(torch.gather(subs[gidx.to(dev)], 1, sig), (0, n - k)))
-            ch_nk.append(torch.full((sel.shape[0],), k, dtype=torch.int32, device=dev))
-            ch_row.append(chunk + n_rows)
-            ch_off.append(off)
-            ch_out.append(sel.to(dev))
-            all_seeds.append(torch.nn.functional.pad(seeds, (0, n - k)))
-            n_rows += seeds.shape[0]
+            groups_k, gidx = torch.unique_consecutive(inv[sel], return_inverse=True)
+            subs = torch.nonzero(kept[groups_k])[:, 1].reshape(-1, k)    # [groups, k] photon ids
+            tab = torch.zeros(sel.shape[0], n + 2, dtype=torch.int64)   # photons | stream id | k
+            tab[:, :k] = subs[gidx]
+            tab[:, n] = sel
+            tab[:, n + 1] = k
+            tabs.append(tab)
             passes.append((k, int(sel.shape[0])))
     s_ids = s_rows = None
     one = kg[inv] == 1
+    C = sum(c for _, c in passes)
+    if C:
+        # the pass draws, pass by pass and chunk by chunk in the reference's order, straight into device
+        # buffers; then the host tables in one copy
+        gdev = _draw_device(generator, dev)
+        R = sum(-(-c // max_streams) for _, c in passes)
+        sig = torch.zeros(C, n, dtype=torch.int64, device=dev)
+        seeds = torch.zeros(R, n, dtype=torch.int64, device=dev)
+        rowoff = torch.empty(C, 2, dtype=torch.int64)                    # seed row | offset in the chunk
+        c0 = r0 = 0
+        for k, cnt in passes:
+            for s0 in range(0, cnt, max_streams):
+                Sc = min(max_streams, cnt - s0)
+                sig[c0 + s0:c0 + s0 + Sc, :k] = torch.argsort(torch.rand(Sc, k, generator=generator, device=gdev),
+                                                              dim=1)
+                seeds[r0, :k] = torch.randint(0, 2 ** 31 - 1, (k,), generator=generator, device=gdev)
+                rowoff[c0 + s0:c0 + s0 + Sc, 0] = r0
+                rowoff[c0 + s0:c0 + s0 + Sc, 1] = torch.arange(Sc)
+                r0 += 1
+            c0 += cnt
+        host = torch.cat([torch.cat(tabs), rowoff], dim=1).to(dev)     # [C, n + 4]
+        nk = host[:, n + 1].to(torch.int32)
+        cols = torch.gather(host[:, :n], 1, sig)
+        cols.masked_fill_(torch.arange(n, device=dev)[None, :] >= nk[:, None], 0)
+        out_row = host[:, n].contiguous()
     if bool(one.any()):
         # streams of the one-photon groups, group by group in sorted order, ascending within a group
         idx = torch.nonzero(one)[:, 0]
@@ -412,13 +431,12 @@ def _plan_loss_only(U, in_modes, S, dp_all, generator, gen, loss, max_streams) -
         photon = torch.nonzero(kept[inv[idx]])[:, 1]
         s_ids = idx.to(dev)
         s_rows = route_lone_photons(U, dp_all[s_ids].cpu(), im_of(in_modes)[photon], generator=gen).to(dev)
-    if not ch_dp:
+    if not C:
         z = torch.zeros(0, dtype=torch.int64, device=dev)
         return ChainPlan(S, n, 0, z, z.reshape(0, n), z.to(torch.int32), z.reshape(0, n), z, z, z, z, s_ids, s_rows, [])
-    nk = torch.cat(ch_nk)
     order = torch.argsort(nk.to(torch.int64), descending=True, stable=True)
-    return ChainPlan(S, n, int(nk.shape[0]), torch.cat(ch_dp), torch.cat(ch_cols), nk, torch.cat(all_seeds),
-                     torch.cat(ch_row), torch.cat(ch_off), torch.cat(ch_out), order, s_ids, s_rows, passes)
+    return ChainPlan(S, n, C, dp_all[out_row], cols, nk, seeds, host[:, n + 2].contiguous(),
+                     host[:, n + 3].contiguous(), out_row, order, s_ids, s_rows, passes)
 
 
 def im_of(in_modes) -> torch.Tensor:
