@@ -143,8 +143,20 @@ def run_reference(args):
             "cpu_baseline": {"value": value, "unit": "samples/s", "cores": threads, "kind": "port",
                              "sample": f"{S} chains per step of the n=20 m=400 workload (bounded sample)"},
             "e2e": {"value": value, "unit": "samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "reference_torch_sampler": reference_torch_sampler()}
+            "reference_torch_sampler": reference_torch_sampler(),
+            "reference_gpu": None if args.no_reference_gpu else reference_engine_gpu()}
     print(json.dumps(line), flush=True)
+
+
+def reference_engine_gpu() -> dict:
+    """The reference's own GPU engine (its public fock_sample, default Triton backend, unmodified, from
+    baseline/_ref) on this machine's GPU at the benchmark workload: 2 000 shots per call, 3 timed calls.
+    Only the reference's code runs here."""
+    import torch
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    U = _haar_dev(M_MODES, USEED, torch.device("cuda"))
+    return public_call_leg([(U, list(range(N_PHOT)))], SHOTS, reps=3, ours=False)
 
 
 def _reference_fock_sample():
