@@ -164,23 +164,57 @@ __device__ __forceinline__ void build_groups_warp(SM& sm, int count) {
 }
 
 // ---------------------------------------------------------------------------------------- plan
+// Value at rank position p (warp-uniform) of a per-lane array holding position lane + 32 q in [q].
+template <int GL, typename T>
+__device__ __forceinline__ T at_position(const T (&v)[GL], int p) {
+    T x = v[0];
+#pragma unroll
+    for (int q = 1; q < GL; ++q)
+        if (p >= 32 * q) x = v[q];
+    return __shfl_sync(0xffffffffu, x, p & 31);
+}
+
+// Exclusive prefix product over rank positions (position lane + 32 q in [q]), in place.
+template <int GL, typename T>
+__device__ __forceinline__ void exclusive_product(T (&v)[GL]) {
+    const int lane = threadIdx.x & 31;
+    T carry = T(1);
+#pragma unroll
+    for (int q = 0; q < GL; ++q) {
+        T x = v[q];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const T y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x *= y;
+        }
+        T ex = __shfl_up_sync(0xffffffffu, x, 1);
+        if (lane == 0) ex = T(1);
+        v[q] = ex * carry;
+        carry *= __shfl_sync(0xffffffffu, x, 31);
+    }
+}
+
 // Warp 0.  Lane g holds group g.  Radix = mult + 1, and one odd-multiplicity group (the last one)
 // has its radix halved to (mult + 1) / 2 with the scale doubled — the complement symmetry
 // v -> s - v of the reference (cofactors_triton.py:428-446); which odd group is halved does not
-// change N or the sum.  Active digits (radix >= 2) are ranked by ascending radix; the leading ones
-// become the Gray lanes (best fill of the CTA's lanes), the next ones the inner block, then the
-// middle block; what does not fit the schedules joins the lanes.
+// change N or the sum.  Active digits (radix >= 2) are ranked by ascending radix (then group); the
+// leading ones become the Gray lanes (best fill of the CTA's lanes), the next ones the inner block, then
+// the middle block; what does not fit the schedules joins the lanes.  The ranking takes one ballot per
+// distinct radix value, and every digit's table entries are written by the lane of its rank, so only
+// the choice of the three splits walks the ranks one by one (in registers, read by shuffles).
 template <class SM>
 __device__ void plan_step(SM& sm, int K1, int K, int lanes, int lin_max, int mid_max) {
     auto& pl = sm.plan;
-    constexpr int GL = (SM::NKMAX + 31) / 32;          // groups per lane: group lane + 32 q, q < GL
+    constexpr int GL = (SM::NKMAX + 31) / 32;          // groups (and ranks) per lane: index lane + 32 q, q < GL
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
     const int D = sm.ngrp;
     int halved = -1;                                   // the last group of odd multiplicity
 #pragma unroll
     for (int q = 0; q < GL; ++q) {
         const int g = lane + 32 * q;
-        const unsigned oddmask = __ballot_sync(0xffffffffu, g < D && (sm.gmul[g < D ? g : 0] & 1));
+        const unsigned oddmask = __ballot_sync(full, g < D && (sm.gmul[g < D ? g : 0] & 1));
         if (oddmask) halved = 32 * q + 31 - __clz(oddmask);
     }
     int R[GL];
@@ -192,94 +226,117 @@ __device__ void plan_step(SM& sm, int K1, int K, int lanes, int lin_max, int mid
         R[q] = g < D ? (g == halved ? (M + 1) / 2 : M + 1) : 1;
         active[q] = R[q] >= 2;
     }
+    // ranks by (radix, group): the groups of the smallest remaining radix take the next ranks in group order
+    unsigned rem[GL];
+#pragma unroll
+    for (int q = 0; q < GL; ++q) rem[q] = __ballot_sync(full, active[q]);
     int na = 0;
+    for (;;) {
+        bool left = false;
 #pragma unroll
-    for (int q = 0; q < GL; ++q) {
-        int rank = 0;                                  // among active groups, by (radix, group)
+        for (int q = 0; q < GL; ++q) left = left || rem[q] != 0u;
+        if (!left) break;                              // warp-uniform: the masks are ballots
+        int mine = 0x7fffffff;
 #pragma unroll
-        for (int q2 = 0; q2 < GL; ++q2) {
-            for (int j = 0; j < 32; ++j) {
-                const int Rj = __shfl_sync(0xffffffffu, R[q2], j);
-                const int gj = j + 32 * q2, g = lane + 32 * q;
-                if (Rj >= 2 && active[q] && (Rj < R[q] || (Rj == R[q] && gj < g))) ++rank;
+        for (int q = 0; q < GL; ++q)
+            if ((rem[q] >> lane) & 1u) mine = min(mine, R[q]);
+        const int rmin = __reduce_min_sync(full, mine);
+#pragma unroll
+        for (int q = 0; q < GL; ++q) {
+            const bool take = ((rem[q] >> lane) & 1u) && R[q] == rmin;
+            const unsigned eq = __ballot_sync(full, take);
+            if (take) {
+                const int r = na + __popc(eq & below);
+                pl.sortR[r] = R[q];
+                pl.sortG[r] = lane + 32 * q;
             }
+            na += __popc(eq);
+            rem[q] &= ~eq;
         }
-        if (active[q]) { pl.sortR[rank] = R[q]; pl.sortG[rank] = lane + 32 * q; }
-        na += __popc(__ballot_sync(0xffffffffu, active[q]));
     }
     __syncwarp();
+    long long rv[GL];                                  // radix at rank position lane + 32 q (1 past na)
+#pragma unroll
+    for (int q = 0; q < GL; ++q) rv[q] = lane + 32 * q < na ? pl.sortR[lane + 32 * q] : 1;
+    long long pre[GL];                                 // product of the radices at positions <= p
+#pragma unroll
+    for (int q = 0; q < GL; ++q) pre[q] = rv[q];
+    exclusive_product<GL>(pre);
+#pragma unroll
+    for (int q = 0; q < GL; ++q) pre[q] *= rv[q];
+    const long long N = na > 0 ? at_position<GL>(pre, na - 1) : 1;
+    // lanes: the prefix of the ranked digits that best fills the CTA's lanes
+    int nhi = na;
+    if (N > lanes) {
+        double best = -1.0;
+        nhi = 1;
+        for (int i = 0; i < na; ++i) {
+            const long long prod = at_position<GL>(pre, i);
+            if (i > 0 && prod > N / 4) break;          // N / prod < 4
+            const double e = prod >= lanes
+                ? (double)prod / ((double)lanes * (double)((prod + lanes - 1) / lanes))
+                : (double)prod / (double)lanes;
+            if (e > best + 1e-12) { best = e; nhi = i + 1; }
+            if (prod >= lanes && e >= 0.95) break;
+        }
+    }
+    int nin = 0, Lin = 1;
+    while (nhi + nin < na) {
+        const int r = (int)at_position<GL>(rv, nhi + nin);
+        if (Lin * r > lin_max) break;
+        Lin *= r;
+        ++nin;
+    }
+    int nmid = 0, Lmid = 1;
+    while (nhi + nin + nmid < na) {
+        const int r = (int)at_position<GL>(rv, nhi + nin + nmid);
+        if (Lmid * r > mid_max) break;
+        Lmid *= r;
+        ++nmid;
+    }
+    // digit order: inner (kd 0..nin-1), middle, lanes, digits beyond both schedules (more lanes), then the
+    // fixed digits (radix 1) in group order; Pin / Pmid the prefix products of the inner / middle radices
+    int pin[GL], pmid[GL];
+#pragma unroll
+    for (int q = 0; q < GL; ++q) {
+        const int p = lane + 32 * q;
+        pin[q] = (p >= nhi && p < nhi + nin) ? (int)rv[q] : 1;
+        pmid[q] = (p >= nhi + nin && p < nhi + nin + nmid) ? (int)rv[q] : 1;
+    }
+    exclusive_product<GL>(pin);
+    exclusive_product<GL>(pmid);
+    int nfix = 0;
+#pragma unroll
+    for (int q = 0; q < GL; ++q) {
+        const int p = lane + 32 * q;
+        if (p < na) {
+            const int g = pl.sortG[p];
+            const int kd = p < nhi ? nin + nmid + p : (p < nhi + nin + nmid ? p - nhi : p);
+            pl.R[kd] = (int)rv[q];
+            pl.M[kd] = sm.gmul[g];
+            pl.drow[kd] = sm.grow[g];
+            if (p >= nhi && p < nhi + nin) pl.Pin[kd] = pin[q];
+            if (p >= nhi + nin && p < nhi + nin + nmid) pl.Pmid[kd - nin] = pmid[q];
+        }
+        const int g = lane + 32 * q;                   // fixed digits: after the active ones, in group order
+        const bool fixed = g < D && !active[q];
+        const unsigned fm = __ballot_sync(full, fixed);
+        if (fixed) {
+            const int kd = na + nfix + __popc(fm & below);
+            pl.R[kd] = 1;
+            pl.M[kd] = sm.gmul[g];
+            pl.drow[kd] = sm.grow[g];
+        }
+        nfix += __popc(fm);
+    }
     if (lane == 0) {
-        int64_t N = 1;
-        for (int i = 0; i < na; ++i) N *= pl.sortR[i];
-        // lanes: the prefix of the ranked digits that best fills the CTA's lanes
-        int nhi = na;
-        if (N > lanes) {
-            double best = -1.0;
-            int64_t prod = 1;
-            nhi = 1;
-            for (int i = 0; i < na; ++i) {
-                prod *= pl.sortR[i];
-                if (i > 0 && N / prod < 4) break;
-                const double e = prod >= lanes
-                    ? (double)prod / ((double)lanes * (double)((prod + lanes - 1) / lanes))
-                    : (double)prod / (double)lanes;
-                if (e > best + 1e-12) { best = e; nhi = i + 1; }
-                if (prod >= lanes && e >= 0.95) break;
-            }
-        }
-        int nin = 0, Lin = 1;
-        while (nhi + nin < na && Lin * pl.sortR[nhi + nin] <= lin_max) { Lin *= pl.sortR[nhi + nin]; ++nin; }
-        int nmid = 0, Lmid = 1;
-        while (nhi + nin + nmid < na && Lmid * pl.sortR[nhi + nin + nmid] <= mid_max) {
-            Lmid *= pl.sortR[nhi + nin + nmid];
-            ++nmid;
-        }
-        const int nextra = na - nhi - nin - nmid;       // digits beyond both schedules: more lanes
-        int kd = 0;
-        for (int i = 0; i < nin; ++i, ++kd) {
-            const int g = pl.sortG[nhi + i];
-            pl.R[kd] = pl.sortR[nhi + i];
-            pl.Pin[kd] = (kd == 0) ? 1 : pl.Pin[kd - 1] * pl.R[kd - 1];
-            pl.M[kd] = sm.gmul[g];
-            pl.drow[kd] = sm.grow[g];
-        }
-        for (int i = 0; i < nmid; ++i, ++kd) {
-            const int g = pl.sortG[nhi + nin + i];
-            pl.R[kd] = pl.sortR[nhi + nin + i];
-            pl.Pmid[i] = (i == 0) ? 1 : pl.Pmid[i - 1] * pl.R[kd - 1];
-            pl.M[kd] = sm.gmul[g];
-            pl.drow[kd] = sm.grow[g];
-        }
-        int64_t H = 1;
-        for (int i = 0; i < nhi; ++i, ++kd) {
-            const int g = pl.sortG[i];
-            pl.R[kd] = pl.sortR[i];
-            pl.M[kd] = sm.gmul[g];
-            pl.drow[kd] = sm.grow[g];
-            H *= pl.R[kd];
-        }
-        for (int i = 0; i < nextra; ++i, ++kd) {
-            const int g = pl.sortG[nhi + nin + nmid + i];
-            pl.R[kd] = pl.sortR[nhi + nin + nmid + i];
-            pl.M[kd] = sm.gmul[g];
-            pl.drow[kd] = sm.grow[g];
-            H *= pl.R[kd];
-        }
-        for (int g = 0; g < D; ++g) {                    // fixed digits: radix 1
-            int Rg = (g == halved) ? (sm.gmul[g] + 1) / 2 : sm.gmul[g] + 1;
-            if (Rg < 2) { pl.R[kd] = 1; pl.M[kd] = sm.gmul[g]; pl.drow[kd] = sm.grow[g]; ++kd; }
-        }
-        pl.N = N; pl.H = H; pl.Lin = Lin; pl.Lmid = Lmid;
+        pl.N = N; pl.H = N / ((long long)Lin * Lmid); pl.Lin = Lin; pl.Lmid = Lmid;
         pl.K = K; pl.K1 = K1; pl.D = D;
-        pl.nin = nin; pl.nmid = nmid; pl.nhi = nhi + nextra;
+        pl.nin = nin; pl.nmid = nmid; pl.nhi = na - nin - nmid;
         pl.scale = (halved >= 0 ? 2.0 : 1.0) * ldexp(1.0, -K1);
     }
 }
 
-// ---------------------------------------------------------------------------------------- prepare
-// One index of a reflected mixed-radix Gray schedule over `nd` digits starting at kernel digit
-// `d0` with radices R and prefix products Pp: its weight prod (-1)^v C(M, v) and the transition
-// into it (the digit the odometer moved, and the sign of the column-sum update -2 dir b).
 template <class PL>
 static __device__ __forceinline__ unsigned char gray_entry(const PL& pl, int d0, int nd, const int* Pp, int t,
                                                           double* w_out, unsigned char* vend, bool binary) {
