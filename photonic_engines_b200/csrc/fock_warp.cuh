@@ -273,11 +273,80 @@ static __device__ double draw_warp_chunks(WarpSmem& sm, const double2* __restric
     return 0.0;
 }
 
-// Four 32-mode chunks at a time when there are many modes (L2 latency hidden by independent loads), one
-// when there are few (four chunks would mostly scan padding: 12-64 modes, 16 % slower).
+// The same draw for at most 32 NCH modes in one pass: every chunk's amplitudes at once (NCH loads of A in
+// flight per column and lane, the columns two at a time), the cumulative weights kept in registers for the
+// pick.  Same sums, scans and comparisons as draw_warp_chunks, so the same bits and the same pick.
+template <int NCH>
+static __device__ double draw_warp_regs(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
+                                        double* __restrict__ marg_row) {
+    const int lane = threadIdx.x & 31;
+    const int nch = (m + 31) >> 5;
+    double xr[NCH], xi[NCH];
+#pragma unroll
+    for (int r = 0; r < NCH; ++r) { xr[r] = 0.0; xi[r] = 0.0; }
+#pragma unroll 2
+    for (int c = 0; c < k; ++c) {
+        const int64_t co = (int64_t)sm.cols[c] * m;
+        const double2 p = sm.P[c];
+        double2 a[NCH];
+#pragma unroll
+        for (int r = 0; r < NCH; ++r) {
+            const int rho = 32 * r + lane;
+            a[r] = (r < nch && rho < m) ? A[(int64_t)rho + co] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int r = 0; r < NCH; ++r) {
+            xr[r] = fma(a[r].x, p.x, xr[r]);
+            xr[r] = fma(-a[r].y, p.y, xr[r]);
+            xi[r] = fma(a[r].x, p.y, xi[r]);
+            xi[r] = fma(a[r].y, p.x, xi[r]);
+        }
+    }
+    double w[NCH], cw[NCH];
+    double carry = 0.0;
+#pragma unroll
+    for (int r = 0; r < NCH; ++r) {
+        const int rho = 32 * r + lane;
+        w[r] = rho < m ? xr[r] * xr[r] + xi[r] * xi[r] : 0.0;
+        cw[r] = 0.0;
+        if (r < nch) {
+            double x = w[r];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            cw[r] = carry + x;
+            carry = __shfl_sync(0xffffffffu, cw[r], 31);
+        }
+    }
+    const double tot = carry, target = u * tot;
+    int cnt = 0;
+    double gmin = 1.0e300;
+#pragma unroll
+    for (int r = 0; r < NCH; ++r) {
+        const int rho = 32 * r + lane;
+        if (r < nch && rho < m) {
+            cnt += (cw[r] < target) ? 1 : 0;
+            gmin = fmin(gmin, fabs(cw[r] - target));
+            if (marg_row) marg_row[rho] = w[r] / tot;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        gmin = fmin(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
+    }
+    if (lane == 0) sm.rows[k - 1] = min(cnt, m - 1);
+    __syncwarp();
+    return gmin / tot;
+}
+
+// Up to 128 modes in one pass with the weights in registers; more in 128-mode pieces scanned twice (L2
+// latency hidden by four chunks' independent loads).
 static __device__ double draw_warp(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
                                    double* __restrict__ marg_row) {
-    return m > 96 ? draw_warp_chunks<4>(sm, A, m, k, u, marg_row) : draw_warp_chunks<1>(sm, A, m, k, u, marg_row);
+    return m > 128 ? draw_warp_chunks<4>(sm, A, m, k, u, marg_row) : draw_warp_regs<4>(sm, A, m, k, u, marg_row);
 }
 
 template <int TPL, int KPW, bool MIXED>
