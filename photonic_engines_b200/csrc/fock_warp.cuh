@@ -2,8 +2,9 @@
 // runs its own stream, so the per-step work (plan, schedules, draw) of many streams proceeds at once
 // and nothing waits on a CTA-wide barrier.  Same algorithm, plan, Gray schedules, all-but-one products,
 // draw rule and uniforms as the CTA form (fock_kernels.cuh); the lanes of the collapsed sum are the
-// warp's 32 / TPL thread groups.  The marginal's CDF is formed in 32-mode chunks twice (once for the
-// total, once for the pick) instead of being stored, so any number of modes fits.
+// warp's 32 / TPL thread groups.  Up to 128 modes the marginal's weights stay in registers and one pass
+// forms the CDF and the pick; beyond, the CDF is formed in 32-mode chunks twice (once for the total, once
+// for the pick) instead of being stored, so any number of modes fits.
 #pragma once
 #include "fock_kernels.cuh"
 
@@ -274,7 +275,7 @@ static __device__ double draw_warp_chunks(WarpSmem& sm, const double2* __restric
 }
 
 // The same draw for at most 32 NCH modes in one pass: every chunk's amplitudes at once (NCH loads of A in
-// flight per column and lane, the columns two at a time), the cumulative weights kept in registers for the
+// flight per column and lane, the columns four at a time), the cumulative weights kept in registers for the
 // pick.  Same sums, scans and comparisons as draw_warp_chunks, so the same bits and the same pick.
 template <int NCH>
 static __device__ double draw_warp_regs(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
@@ -284,7 +285,7 @@ static __device__ double draw_warp_regs(WarpSmem& sm, const double2* __restrict_
     double xr[NCH], xi[NCH];
 #pragma unroll
     for (int r = 0; r < NCH; ++r) { xr[r] = 0.0; xi[r] = 0.0; }
-#pragma unroll 2
+#pragma unroll 4
     for (int c = 0; c < k; ++c) {
         const int64_t co = (int64_t)sm.cols[c] * m;
         const double2 p = sm.P[c];
@@ -342,10 +343,11 @@ static __device__ double draw_warp_regs(WarpSmem& sm, const double2* __restrict_
     return gmin / tot;
 }
 
-// Up to 128 modes in one pass with the weights in registers; more in 128-mode pieces scanned twice (L2
-// latency hidden by four chunks' independent loads).
+// Up to 128 modes in one pass with the weights in registers (two chunks' registers up to 64 modes); more
+// in 128-mode pieces scanned twice (L2 latency hidden by four chunks' independent loads).
 static __device__ double draw_warp(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
                                    double* __restrict__ marg_row) {
+    if (m <= 64) return draw_warp_regs<2>(sm, A, m, k, u, marg_row);
     return m > 128 ? draw_warp_chunks<4>(sm, A, m, k, u, marg_row) : draw_warp_regs<4>(sm, A, m, k, u, marg_row);
 }
 
