@@ -343,12 +343,99 @@ static __device__ double draw_warp_regs(WarpSmem& sm, const double2* __restrict_
     return gmin / tot;
 }
 
-// Up to 128 modes in one pass with the weights in registers (two chunks' registers up to 64 modes); more
-// in 128-mode pieces scanned twice (L2 latency hidden by four chunks' independent loads).
+// Weights and inclusive CDF of one piece of 32 DRW modes from `carry` (the CDF before the piece), as
+// draw_warp_chunks forms them; returns the CDF at the piece's end.
+template <int DRW>
+static __device__ __forceinline__ double draw_piece(const WarpSmem& sm, const double2* __restrict__ A, int m, int k,
+                                                    int base, double carry, double (&w)[DRW], double (&cw)[DRW]) {
+    const int lane = threadIdx.x & 31;
+    double xr[DRW], xi[DRW];
+#pragma unroll
+    for (int r = 0; r < DRW; ++r) { xr[r] = 0.0; xi[r] = 0.0; }
+#pragma unroll 2
+    for (int c = 0; c < k; ++c) {
+        const int64_t co = (int64_t)sm.cols[c] * m;
+        const double2 p = sm.P[c];
+        double2 a[DRW];
+#pragma unroll
+        for (int r = 0; r < DRW; ++r) {
+            const int rho = base + 32 * r + lane;
+            a[r] = rho < m ? A[(int64_t)rho + co] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int r = 0; r < DRW; ++r) {
+            xr[r] = fma(a[r].x, p.x, xr[r]);
+            xr[r] = fma(-a[r].y, p.y, xr[r]);
+            xi[r] = fma(a[r].x, p.y, xi[r]);
+            xi[r] = fma(a[r].y, p.x, xi[r]);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < DRW; ++r) {
+        const int rho = base + 32 * r + lane;
+        w[r] = rho < m ? xr[r] * xr[r] + xi[r] * xi[r] : 0.0;
+        double x = w[r];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        cw[r] = carry + x;
+        carry = __shfl_sync(0xffffffffu, cw[r], 31);
+    }
+    return carry;
+}
+
+// The draw for 129 to 4096 modes without a second full pass: the first pass keeps the CDF at the end of
+// every 128-mode piece (piece p in lane p), the pick's piece is the first whose end reaches u tot, and only
+// that piece is formed again (the same sums from the same carry, so the same bits).  The CDF grows
+// monotonically from piece to piece (non-negative weights added to the carry), so every mode of an earlier
+// piece lies below u tot and none of a later one does: the count, and the distance of the CDF to u tot
+// (at the pick's piece and at the end of the piece before it), are those of the full scan.
+static __device__ double draw_warp_pieces(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u) {
+    constexpr int DRW = 4, PIECE = 32 * DRW;
+    const int lane = threadIdx.x & 31;
+    const int np = (m + PIECE - 1) / PIECE;
+    double w[DRW], cw[DRW];
+    double carry = 0.0, mine = 0.0;
+    for (int pc = 0; pc < np; ++pc) {
+        carry = draw_piece<DRW>(sm, A, m, k, pc * PIECE, carry, w, cw);
+        if (lane == pc) mine = carry;
+    }
+    const double tot = carry, target = u * tot;
+    const unsigned reach = __ballot_sync(0xffffffffu, lane < np && mine >= target);
+    const int j = reach ? __ffs(reach) - 1 : np - 1;
+    const double prev = __shfl_sync(0xffffffffu, mine, j > 0 ? j - 1 : 0);
+    draw_piece<DRW>(sm, A, m, k, j * PIECE, j > 0 ? prev : 0.0, w, cw);
+    int cnt = 0;
+    double gmin = j > 0 ? fabs(prev - target) : 1.0e300;
+#pragma unroll
+    for (int r = 0; r < DRW; ++r) {
+        const int rho = j * PIECE + 32 * r + lane;
+        if (rho < m) {
+            cnt += (cw[r] < target) ? 1 : 0;
+            gmin = fmin(gmin, fabs(cw[r] - target));
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        gmin = fmin(gmin, __shfl_xor_sync(0xffffffffu, gmin, o));
+    }
+    if (lane == 0) sm.rows[k - 1] = min(j * PIECE + cnt, m - 1);
+    __syncwarp();
+    return gmin / tot;
+}
+
+// Up to 128 modes in one pass with the weights in registers (two chunks' registers up to 64 modes); up to
+// 4096 in 128-mode pieces with only the pick's piece formed twice; beyond, or when the marginal itself is
+// asked for, the whole CDF scanned twice (L2 latency hidden by four chunks' independent loads).
 static __device__ double draw_warp(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
                                    double* __restrict__ marg_row) {
     if (m <= 64) return draw_warp_regs<2>(sm, A, m, k, u, marg_row);
-    return m > 128 ? draw_warp_chunks<4>(sm, A, m, k, u, marg_row) : draw_warp_regs<4>(sm, A, m, k, u, marg_row);
+    if (m <= 128) return draw_warp_regs<4>(sm, A, m, k, u, marg_row);
+    if (!marg_row && m <= 32 * 128) return draw_warp_pieces(sm, A, m, k, u);
+    return draw_warp_chunks<4>(sm, A, m, k, u, marg_row);
 }
 
 template <int TPL, int KPW, bool MIXED>

@@ -159,6 +159,22 @@ def test_chains_match_the_oracle_with_supplied_uniforms(n, m, S, mode):
             assert _rel(mmx[s, k], ref["marg"][s, k]) <= mixed_tol(k + 1)
 
 
+@pytest.mark.parametrize("n,m,S", [(10, 300, 48), (12, 900, 32), (6, 4200, 16)])
+def test_warp_form_picks_over_many_modes_match_the_oracle(n, m, S):
+    """The warp form's draw over more than 128 modes without the marginal output (the CDF kept at every
+    128-mode piece, only the pick's piece formed again; past 4096 modes the whole CDF scanned twice): rows
+    bit-exact against the oracle where its draws are far from a CDF step, the mixed form's picks equal."""
+    U, sig, u = _random_chains(n, m, S, 2000 + m)
+    ref = O.chain(U[:, :n], np.zeros(S, np.int64), sig, u, marg=False)
+    Ut = torch.tensor(U, device=DEV)
+    rows = sample_chains(Ut, list(range(n)), sig, uniforms=u, mode="warp")["rows"].cpu().numpy()
+    mix = sample_chains(Ut, list(range(n)), sig, uniforms=u, mode="warp", precision="mixed")["rows"].cpu().numpy()
+    far = (ref["gap"] > 1e-11).all(axis=1)
+    assert far.mean() > 0.9
+    assert np.array_equal(rows[far], ref["rows"][far])
+    assert np.array_equal(mix, rows)
+
+
 def f64_tol(k: int) -> float:
     """FP64 envelope at a step with k columns: 1e-10 up to 24, growing 1.8x per column beyond (sums of
     2^(k-2) terms; the FP64 oracle itself sits 1.9e-10 from its long-double form at k = 29)."""
