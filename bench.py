@@ -836,6 +836,7 @@ PUBLISHED = [
     ("s/sample n=36 m=2n", 36, 72, 8, None, 0.23, "s/sample", "docs/ALGORITHMS.md:186-194"),
     ("s/sample n=38 m=2n", 38, 76, 4, None, 0.84, "s/sample", "docs/ALGORITHMS.md:186-194"),
     ("s/sample n=40 m=2n", 40, 80, 4, None, 2.6, "s/sample", "docs/ALGORITHMS.md:186-194"),
+    ("samples/s k=6 m=12 plateau", 6, 12, 65536, None, 45.3e6, "samples/s", "results/keep/cost_table_20261011_h100.csv"),
     ("samples/s k=20 m=24", 20, 24, 4096, None, 108.0e3, "samples/s", "results/keep/cost_table_20261011_h100.csv"),
     ("samples/s k=20 m=32", 20, 32, 4096, None, 74.6e3, "samples/s", "results/keep/cost_table_20261011_h100.csv"),
     ("samples/s k=20 m=48", 20, 48, 4096, None, 45.1e3, "samples/s", "results/keep/cost_table_20261011_h100.csv"),
