@@ -883,7 +883,10 @@ def run_published(args):
         kw = {} if loss is None else {"loss": loss}
         fock_sample(U, list(range(n)), shots, generator=gen, **kw)
         torch.cuda.synchronize()
-        reps = max(1, args.steps // 2)
+        t0 = time.perf_counter()
+        fock_sample(U, list(range(n)), shots, generator=gen, **kw)     # second warm call, timed: sizes reps
+        torch.cuda.synchronize()
+        reps = max(1, args.steps // 2, int(0.3 / max(time.perf_counter() - t0, 1e-6)))   # >= ~0.3 s per row
         t0 = time.perf_counter()
         for _ in range(reps):
             fock_sample(U, list(range(n)), shots, generator=gen, **kw)
