@@ -30,13 +30,15 @@ static void* g_cof[N_PREC][3][N_KPM];
 static void* g_split_partial[N_PREC][3][N_KPM];
 static void* g_split_draw[N_PREC][3][N_KPM];
 static void* g_warp[N_PREC][3][N_KPM];
+static size_t g_warp_slice[N_PREC][3][N_KPM];
 static bool prec_ok(int p) { return p >= 0 && p < N_PREC; }
 
 void register_variant(int mixed, int tpl, int kpm, void* chain_kernel, void* cofactor_kernel, void* split_partial,
-                      void* split_draw, void* warp_kernel) {
+                      void* split_draw, void* warp_kernel, size_t warp_slice_bytes) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
     if (!prec_ok(mixed) || ti < 0 || ki < 0) return;
     g_warp[mixed][ti][ki] = warp_kernel;
+    g_warp_slice[mixed][ti][ki] = warp_slice_bytes;
     g_chain[mixed][ti][ki] = chain_kernel;
     g_cof[mixed][ti][ki] = cofactor_kernel;
     g_split_partial[mixed][ti][ki] = split_partial;
@@ -50,7 +52,11 @@ void* find_warp_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
     return (!prec_ok(mixed) || ti < 0 || ki < 0) ? nullptr : g_warp[mixed][ti][ki];
 }
-size_t warp_smem_bytes(int warps) { return sizeof(WarpSmem) * (size_t)warps; }
+size_t warp_smem_bytes(int mixed, int tpl, int kpm, int warps) {
+    const int ti = tpl_index(tpl), ki = kpm_index(kpm);
+    const size_t slice = (!prec_ok(mixed) || ti < 0 || ki < 0) ? 0 : g_warp_slice[mixed][ti][ki];
+    return (slice ? slice : sizeof(WarpSmem)) * (size_t)warps;
+}
 void* find_split_draw_kernel(int mixed, int tpl, int kpm) {
     const int ti = tpl_index(tpl), ki = kpm_index(kpm);
     return (!prec_ok(mixed) || ti < 0 || ki < 0) ? nullptr : g_split_draw[mixed][ti][ki];
@@ -280,7 +286,7 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     if (kpm > NARROW && precision != PE_PRECISION_F64) return PE_ERR_SIZE;   // mixed form: up to 32 columns
     if (warp_mode && (kpm > WMAXN || split || precision == PE_PRECISION_COMPENSATED)) return PE_ERR_SIZE;
     if (tpl == 0) {
-        tpl = warp_mode ? (kpm <= 8 ? 1 : 2) : default_tpl(kpm, precision);
+        tpl = warp_mode ? 2 : default_tpl(kpm, precision);     // warp form: two-thread lanes (8 columns: three CTAs per SM)
         if (!warp_mode && !find_chain_kernel(precision, tpl, kpm)) tpl = find_chain_kernel(precision, 2, kpm) ? 2 : 4;
     }
     if (tpl_index(tpl) < 0) return PE_ERR_ARG;
@@ -296,7 +302,8 @@ static int chain_launch(int precision, const double* d_acol, const int64_t* d_in
     if (block < 32 || block > 256 || block > bmax || (block & 31)) return PE_ERR_ARG;
     if (!warp_mode && block < ncols) return PE_ERR_ARG;
     const size_t smem_fix = smem_fixed_bytes_for(kpm, precision);
-    const size_t smem = warp_mode ? warp_smem_bytes(block / 32) : smem_fix + (size_t)m_max * sizeof(double);
+    const size_t smem = warp_mode ? warp_smem_bytes(precision, tpl, kpm, block / 32)
+                                  : smem_fix + (size_t)m_max * sizeof(double);
     const int cap = max_smem_optin();
     if (cap <= 0) return PE_ERR_CUDA;
     if (smem > (size_t)cap) return PE_ERR_SIZE;

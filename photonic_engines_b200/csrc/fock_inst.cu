@@ -18,9 +18,10 @@ struct Registration {
                              (void*)pe::split_partial_kernel<PE_TPL, PE_KPM, PE_MIXED>,
                              (void*)pe::split_draw_kernel<PE_TPL, PE_KPM, PE_MIXED>,
 #if PE_KPM <= 16 && PE_TPL <= 2 && PE_MIXED <= 1
-                             (void*)pe::fock_chain_warp_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>
+                             (void*)pe::fock_chain_warp_kernel<PE_TPL, PE_KPM, (PE_MIXED != 0)>,
+                             sizeof(pe::WarpSmemT<PE_KPM>)
 #else
-                             nullptr
+                             nullptr, 0
 #endif
         );
     }

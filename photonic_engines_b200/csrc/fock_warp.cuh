@@ -15,49 +15,53 @@ constexpr int WLIN = 128;      // inner schedule length
 constexpr int WMID = 128;      // middle schedule length
 constexpr int WARPS = 8;       // warps (streams in flight) per CTA
 
-struct WarpSmem {
-    static constexpr int NKMAX = WMAXN;
-    Plan plan;
-    double2 P[WMAXN];
-    double2 B[WMAXN][WMAXN];
-    float2 B32[WMAXN][WMAXN];
+template <int NK>
+struct WarpSmemT {
+    static constexpr int NKMAX = NK;
+    PlanT<NK> plan;
+    double2 P[NK];
+    double2 B[NK][NK];
+    float2 B32[NK][NK];
     double tab_w[WLIN];
     float tab_w32[WLIN];
     double tab_wm[WMID];
     unsigned char tab_f[WLIN];
     unsigned char tab_fm[WMID];
-    int rows[WMAXN];
-    int cols[WMAXN];
-    int grow[WMAXN];
-    int gmul[WMAXN];
+    int rows[NK];
+    int cols[NK];
+    int grow[NK];
+    int gmul[NK];
     int ngrp;
     int bad;
     int64_t cur;
     int64_t lane0;
     int lane_mult;
 };
+using WarpSmem = WarpSmemT<WMAXN>;    // the largest slice (streams of up to 16 photons)
 
 // Gather B and fill the schedules, lane-parallel.  Element (rho, j) of the instance is A[rho + j * m].
-static __device__ void prepare_warp(WarpSmem& sm, const double2* __restrict__ A, int m, bool mixed) {
-    const Plan& pl = sm.plan;
+template <class WS>
+static __device__ void prepare_warp(WS& sm, const double2* __restrict__ A, int m, bool mixed) {
+    constexpr int NW = WS::NKMAX;
+    const auto& pl = sm.plan;
     const int lane = threadIdx.x & 31;
     // the gather from L2 with GB independent loads in flight per lane before any store
     constexpr int GB = 8;
-    const int nel = pl.D * WMAXN;
+    const int nel = pl.D * NW;
     for (int base = lane; base < nel; base += 32 * GB) {
         double2 v[GB];
 #pragma unroll
         for (int g = 0; g < GB; ++g) {
             const int idx = base + 32 * g;
-            const bool ok = idx < nel && idx % WMAXN < pl.K;
-            const int kd = ok ? idx / WMAXN : 0, j = ok ? idx % WMAXN : 0;     // in range even when not loaded
+            const bool ok = idx < nel && idx % NW < pl.K;
+            const int kd = ok ? idx / NW : 0, j = ok ? idx % NW : 0;     // in range even when not loaded
             v[g] = ok ? A[(int64_t)pl.drow[kd] + (int64_t)sm.cols[j] * m] : make_double2(0.0, 0.0);
         }
 #pragma unroll
         for (int g = 0; g < GB; ++g) {
             const int idx = base + 32 * g;
             if (idx < nel) {
-                const int kd = idx / WMAXN, j = idx % WMAXN;
+                const int kd = idx / NW, j = idx % NW;
                 sm.B[kd][j] = v[g];
                 if (mixed) sm.B32[kd][j] = make_float2((float)(2.0 * v[g].x), (float)(2.0 * v[g].y));
             }
@@ -81,8 +85,8 @@ static __device__ void prepare_warp(WarpSmem& sm, const double2* __restrict__ A,
 
 // Sum of the warp's lane accumulators (all lanes of a thread position hold the same total), times the
 // scale, into sm.P.
-template <int KH, int TPL>
-__device__ __forceinline__ void reduce_warp_to_P(double (&ar)[KH], double (&ai)[KH], WarpSmem& sm, int c0) {
+template <int KH, int TPL, class WS>
+__device__ __forceinline__ void reduce_warp_to_P(double (&ar)[KH], double (&ai)[KH], WS& sm, int c0) {
     const int lane = threadIdx.x & 31;
     __syncwarp();
 #pragma unroll
@@ -101,10 +105,10 @@ __device__ __forceinline__ void reduce_warp_to_P(double (&ar)[KH], double (&ai)[
     __syncwarp();
 }
 
-template <int KP, int TPL>
-__device__ void sweep_warp_f64(WarpSmem& sm) {
+template <int KP, int TPL, class WS>
+__device__ void sweep_warp_f64(WS& sm) {
     constexpr int KH = KP / TPL;
-    const Plan& pl = sm.plan;
+    const auto& pl = sm.plan;
     const int lane_id = threadIdx.x & 31;
     const int lanes = 32 / TPL, lane = lane_id / TPL, h = lane_id % TPL, c0 = h * KH;
     const unsigned gmask = 0xffffffffu;                    // the warp walks its lanes in lockstep
@@ -139,10 +143,10 @@ __device__ void sweep_warp_f64(WarpSmem& sm) {
     reduce_warp_to_P<KH, TPL>(ar, ai, sm, c0);
 }
 
-template <int KP, int TPL>
-__device__ void sweep_warp_mixed(WarpSmem& sm) {
+template <int KP, int TPL, class WS>
+__device__ void sweep_warp_mixed(WS& sm) {
     constexpr int KH = KP / TPL;
-    const Plan& pl = sm.plan;
+    const auto& pl = sm.plan;
     const int lane_id = threadIdx.x & 31;
     const int lanes = 32 / TPL, lane = lane_id / TPL, h = lane_id % TPL, c0 = h * KH;
     const unsigned gmask = 0xffffffffu;
@@ -189,8 +193,8 @@ __device__ void sweep_warp_mixed(WarpSmem& sm) {
         if (K <= KPv) { CALL; return; }                      \
     }
 
-template <int TPL, int KPW, bool MIXED>
-__device__ void warp_cofactors(WarpSmem& sm, int K) {
+template <int TPL, int KPW, bool MIXED, class WS>
+__device__ void warp_cofactors(WS& sm, int K) {
     if constexpr (MIXED) {
         PE_WTIER(4, (sweep_warp_mixed<4, TPL>(sm)))
         PE_WTIER(8, (sweep_warp_mixed<8, TPL>(sm)))
@@ -206,8 +210,8 @@ __device__ void warp_cofactors(WarpSmem& sm, int K) {
 
 // Marginal, CDF and pick of one step (the rule of cofactors_triton.py:298-308, tot = cw[m - 1]); the
 // 32-mode chunks are scanned twice.  Returns min |cw - u tot| / tot.
-template <int DRW>
-static __device__ double draw_warp_chunks(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
+template <int DRW, class WS>
+static __device__ double draw_warp_chunks(WS& sm, const double2* __restrict__ A, int m, int k, double u,
                                           double* __restrict__ marg_row) {
     const int lane = threadIdx.x & 31;
     double tot = 0.0;
@@ -277,8 +281,8 @@ static __device__ double draw_warp_chunks(WarpSmem& sm, const double2* __restric
 // The same draw for at most 32 NCH modes in one pass: every chunk's amplitudes at once (NCH loads of A in
 // flight per column and lane, the columns four at a time), the cumulative weights kept in registers for the
 // pick.  Same sums, scans and comparisons as draw_warp_chunks, so the same bits and the same pick.
-template <int NCH>
-static __device__ double draw_warp_regs(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
+template <int NCH, class WS>
+static __device__ double draw_warp_regs(WS& sm, const double2* __restrict__ A, int m, int k, double u,
                                         double* __restrict__ marg_row) {
     const int lane = threadIdx.x & 31;
     const int nch = (m + 31) >> 5;
@@ -345,8 +349,8 @@ static __device__ double draw_warp_regs(WarpSmem& sm, const double2* __restrict_
 
 // Weights and inclusive CDF of one piece of 32 DRW modes from `carry` (the CDF before the piece), as
 // draw_warp_chunks forms them; returns the CDF at the piece's end.
-template <int DRW>
-static __device__ __forceinline__ double draw_piece(const WarpSmem& sm, const double2* __restrict__ A, int m, int k,
+template <int DRW, class WS>
+static __device__ __forceinline__ double draw_piece(const WS& sm, const double2* __restrict__ A, int m, int k,
                                                     int base, double carry, double (&w)[DRW], double (&cw)[DRW]) {
     const int lane = threadIdx.x & 31;
     double xr[DRW], xi[DRW];
@@ -392,7 +396,8 @@ static __device__ __forceinline__ double draw_piece(const WarpSmem& sm, const do
 // monotonically from piece to piece (non-negative weights added to the carry), so every mode of an earlier
 // piece lies below u tot and none of a later one does: the count, and the distance of the CDF to u tot
 // (at the pick's piece and at the end of the piece before it), are those of the full scan.
-static __device__ double draw_warp_pieces(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u) {
+template <class WS>
+static __device__ double draw_warp_pieces(WS& sm, const double2* __restrict__ A, int m, int k, double u) {
     constexpr int DRW = 4, PIECE = 32 * DRW;
     const int lane = threadIdx.x & 31;
     const int np = (m + PIECE - 1) / PIECE;
@@ -430,7 +435,8 @@ static __device__ double draw_warp_pieces(WarpSmem& sm, const double2* __restric
 // Up to 128 modes in one pass with the weights in registers (two chunks' registers up to 64 modes); up to
 // 4096 in 128-mode pieces with only the pick's piece formed twice; beyond, or when the marginal itself is
 // asked for, the whole CDF scanned twice (L2 latency hidden by four chunks' independent loads).
-static __device__ double draw_warp(WarpSmem& sm, const double2* __restrict__ A, int m, int k, double u,
+template <class WS>
+static __device__ double draw_warp(WS& sm, const double2* __restrict__ A, int m, int k, double u,
                                    double* __restrict__ marg_row) {
     if (m <= 64) return draw_warp_regs<2>(sm, A, m, k, u, marg_row);
     if (m <= 128) return draw_warp_regs<4>(sm, A, m, k, u, marg_row);
@@ -438,8 +444,8 @@ static __device__ double draw_warp(WarpSmem& sm, const double2* __restrict__ A, 
     return draw_warp_chunks<4>(sm, A, m, k, u, marg_row);
 }
 
-template <int TPL, int KPW, bool MIXED>
-__device__ void chain_warp(const ChainParams& p, WarpSmem& sm, int64_t s) {
+template <int TPL, int KPW, bool MIXED, class WS>
+__device__ void chain_warp(const ChainParams& p, WS& sm, int64_t s) {
     const int lane = threadIdx.x & 31;
     const int64_t g = p.dp[s];
     bool ok = g >= 0 && g < p.G;
@@ -513,10 +519,16 @@ __device__ void chain_warp(const ChainParams& p, WarpSmem& sm, int64_t s) {
     __syncwarp();
 }
 
+// Two-thread lanes of at most 8 columns fit 80 registers and a 5 KB slice per stream: three CTAs per SM
+// (24 streams in flight instead of 16); the others keep two.
+template <int TPL, int KPW>
+constexpr int warp_ctas_per_sm() { return (KPW <= 8 && TPL == 2) ? 3 : 2; }
+
 template <int TPL, int KPW, bool MIXED>
-__global__ void __launch_bounds__(32 * WARPS, 2) fock_chain_warp_kernel(ChainParams p) {
+__global__ void __launch_bounds__(32 * WARPS, warp_ctas_per_sm<TPL, KPW>()) fock_chain_warp_kernel(ChainParams p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    WarpSmem& sm = reinterpret_cast<WarpSmem*>(smem_raw)[threadIdx.x >> 5];
+    using WS = WarpSmemT<KPW>;
+    WS& sm = reinterpret_cast<WS*>(smem_raw)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     for (;;) {
         if (lane == 0) {
