@@ -30,6 +30,7 @@ def _resident_split_ctas(device, precision: str, n: int, tpl: int) -> int:
     return _split_slots(dev.index if dev.index is not None else torch.cuda.current_device(), precision, n, 128, tpl)
 
 DEFAULT_CUTS = (20, 16)
+WARP_SMALL = 8                 # warp-form batches: chains of at most this many photons get their own tier
 LONG_SPLIT_ABOVE = 24          # chains longer than this get their own tier with split steps
 # tier cut points the autotuner tries (descending; the last tier <= 16 photons runs in the warp form)
 CUT_CANDIDATES = [(20, 16), (24, 16), (20, 12), (24, 20, 16), (16,), (20, 16, 12)]
@@ -122,11 +123,14 @@ class BatchedSampler:
         # replays the cut for every batch; the autotuner may pick other cut points
         varied = self.singles or any(e < 1.0 for e in etas) or len(set(self.n)) > 1
         self.tiered = bool(tiers and varied and not self.warp and not self.split and self.n_stride > WARP_MAX_PHOTONS)
+        # short chains of several lengths, all in the warp form: those of at most 8 photons in the 8-column
+        # kernel (smaller shared-memory slices, three CTAs per SM), the rest in the batch's own
+        self.warp_tiered = bool(tiers and varied and self.warp and self.n_stride > WARP_SMALL)
         self.wsb = int(N.load().pe_chain_workspace_bytes(C))
         self.qr_all = torch.tensor([0, C], dtype=torch.int64, device=dev)      # the whole queue (warp form)
         self.tier_ws, self._side_streams = [], []
         self.long_split = self._plan_long_split(etas, xs) if self.tiered else None
-        self._set_tiers(DEFAULT_CUTS if self.tiered else ())
+        self._set_tiers(DEFAULT_CUTS if self.tiered else ((WARP_SMALL,) if self.warp_tiered else ()))
         self.gen = torch.Generator(device=dev).manual_seed(seed)
         self._row0 = [0]
         for s_ in shots_l:
@@ -153,7 +157,8 @@ class BatchedSampler:
         if not cuts:
             return
         last_warp = 1 if (cuts[-1] <= WARP_MAX_PHOTONS and self.precision != "compensated") else 0
-        self.tiers = [(self.n_stride, 0)] + [(c, 0) for c in cuts[:-1]] + [(cuts[-1], last_warp)]
+        top = 1 if self.warp else 0                      # a warp-form batch keeps its longest chains in it too
+        self.tiers = [(self.n_stride, top)] + [(c, 0) for c in cuts[:-1]] + [(cuts[-1], last_warp)]
         if self.long_split is not None:                  # the longest chains: their own tier, steps split
             lim = self.long_split["above"]
             self.tiers = [(self.n_stride, 2)] + [t for t in self.tiers if t[0] < lim]
@@ -234,7 +239,9 @@ class BatchedSampler:
             for i, (nk_max, mode) in enumerate(self.tiers):
                 stream = cur if i == 0 else self.tier_streams[i - 1]
                 b, t = (block, tpl) if i == 0 else (0, 0)          # the tuned shape is the top tier's
-                if mode == 1:
+                if mode == 1 and i == 0:                          # a warp-form batch's longest chains
+                    t = tpl if tpl in (1, 2) else 0
+                elif mode == 1:
                     b, t = self.warp_block, 0
                 if mode == 2:
                     ls = self.long_split
