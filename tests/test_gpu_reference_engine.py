@@ -142,3 +142,13 @@ def test_emitter_caterpillar(ref_emitter, kw):
     a = ref_fn(rst, U, 256, generator=torch.Generator().manual_seed(31), **kw)
     b = emitter_sample(st, U, 256, generator=torch.Generator().manual_seed(31), **kw)
     assert torch.equal(a.cpu(), b.cpu())
+
+
+def test_lossy_call_with_long_survivors_runs_the_split_tier(ref):
+    """n_in = 30, m = 900 at transmission 0.9: most survivors have more than 24 photons, so the call's longest
+    tier runs with split steps (kernels.tier_plan mode 2) beside the 21-24- and 17-20-photon tiers."""
+    from photonic_engines_b200.clifford import kernels as K
+    U = torch.tensor(O.haar_unitary(900, 3002), device=DEV)
+    tiers = K.tier_plan({27: 20, 26: 10, 23: 5, 19: 2}, 30, "f64", torch.device(DEV))
+    assert tiers[0][3] == 2
+    _same(ref, U, list(range(30)), 48, 25, loss=0.9)

@@ -117,3 +117,21 @@ def test_split_plan_sizes_the_ctas_per_stream_from_the_resident_slots(monkeypatc
     assert heavy * nch >= waves * slots or nch == min(K.NCH_MAX, (1 << (n - 2)) // (32 * 128))
     assert (1 << (k - 2)) >= 4 * nch * 128 and (1 << (k - 3)) < 4 * nch * 128
     assert (k, nch) == expect
+
+
+def test_tier_plan_cuts_the_longest_first_queue(monkeypatch):
+    """Length tiers of a ragged call on the CPU (resident split CTAs stubbed): consecutive queue ranges,
+    longest first; the few chains above 24 photons split, a crowd of them not; the last tier in the warp form
+    only when its streams fill the GPU's warps."""
+    from photonic_engines_b200.clifford import kernels as K
+    monkeypatch.setattr(K, "_split_slots", lambda *a: 296)
+    monkeypatch.setattr(K, "use_warp_form", lambda S, n, d: n <= 12 or S >= 64 * 148)
+    t = K.tier_plan({27: 3, 25: 2, 22: 40, 18: 500, 15: 3000, 9: 100}, 30, "f64", "cuda:0")
+    assert [(a, b, k, mode) for a, b, k, mode, _ in t] == [(0, 5, 27, 2), (5, 45, 22, 0), (45, 545, 18, 0),
+                                                          (545, 3645, 15, 0)]
+    assert t[0][4] is not None
+    t = K.tier_plan({27: 5000, 22: 10}, 30, "f64", "cuda:0")
+    assert t[0][3] == 0 and t[0][4] is None                     # enough long chains to fill the GPU whole
+    t = K.tier_plan({12: 100, 7: 50}, 12, "f64", "cuda:0")
+    assert t == [(0, 150, 12, 1, None)]                          # one tier: the plain launch runs it
+    assert K.tier_plan({}, 30, "f64", "cuda:0") == []
