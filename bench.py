@@ -646,6 +646,29 @@ def profile_launch(precision: str):
     torch.cuda.synchronize()
 
 
+def profile_batch(name: str):
+    """Three warm-up batches and two timed batches of a configuration through the batched sampler in FP64,
+    launched eagerly (no CUDA graph, default launch shapes) so that a profiler sees every tier's launch."""
+    import torch
+
+    from photonic_engines_b200.clifford import BatchedSampler
+    dev = torch.device("cuda", 0)
+    circuits, shots, loss, indist, _ = _config_circuits(name, dev)
+    bs = BatchedSampler(circuits, shots, loss=loss, indist=indist, precision="f64", seed=7, tune=False, graph=False)
+    for _ in range(3):
+        bs.sample()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(2):
+        bs.sample()
+    e1.record()
+    torch.cuda.synchronize()
+    bs.check()
+    print(json.dumps({"config": name, "ms_per_batch": e0.elapsed_time(e1) / 2, "tiers": bs.tiers,
+                      "chains": bs.C}), flush=True)
+
+
 def run_emitter(args):
     """One JSON line for EmitterMPS inputs: the linear cluster state (caterpillar, spin_gate(pi/2, 0) at every
     emission, emitter traced out) of n = 12 photons in m = 24 modes through a seeded Haar U, 512 shots per step
@@ -953,9 +976,14 @@ def main():
                     help="c2 (default) is the headline line; c1 c3 c4 c5 run through the batched sampler, emitter "
                          "the EmitterMPS path, single the one-sample latency path, adaptive prefix / avoid, published "
                          "the workloads of the reference's published H100 numbers")
+    ap.add_argument("--profile-batch", choices=("c1", "c3", "c4", "c5"), default=None,
+                    help="run only five eager FP64 batches of a configuration (a target for an ncu launch list)")
     ap.add_argument("--profile-launch", choices=FORMS, default=None,
                     help="run only two chain launches of the workload (a target for ncu -s 1 -c 1)")
     args = ap.parse_args()
+    if args.profile_batch:
+        profile_batch(args.profile_batch)
+        return
     if args.profile_launch:
         profile_launch(args.profile_launch)
         return
